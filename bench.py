@@ -1,0 +1,338 @@
+"""Benchmark of the fill-path symbolic factorization on B200.
+
+One step = one full symbolic factorization (every source row, both halves
+of L+U, supernode detection) of the circuit-like matrix n=659,033 with
+~5.84M nonzeros (the reference's pre2 test graph shape; seeded synthetic
+stand-in), max supernode size 128.
+
+  value   fill-path GTEPS = edges_alg / device time, inputs resident in HBM
+  e2e     the same metric through the C-ABI with host buffers: H2D of the
+          CSR, device ingest/transpose, factorization, D2H of the per-row
+          counts, every step
+  roofline  traversal kernel: algorithmic bytes (8*E_alg + 16*V_alg +
+          4*W_out) per launch / its CUDA-event duration vs measured HBM peak
+
+Usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+N > 1 runs under torchrun as independent replicas (one matrix per GPU, no
+collective on the data path); value = all ranks' edges / max-over-ranks time.
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WORKLOADS = {
+    "circuit_like": "circuit-like n=659033 ~5.84M nnz, Zipf(1.2) long links, symmetric permutation, mss 128",
+    "random_extra": "n=20000 diagonal+tridiagonal+3 uniform columns/row, mss 128",
+    "grid3d_64": "64^3 7-point grid, nested-dissection order, mss 256",
+}
+
+
+def make_workload(name):
+    from gsofatpds_b200 import gen
+    if name == "circuit_like":
+        return gen.circuit_like(), 128
+    if name == "random_extra":
+        return gen.random_extra(20000, 3, seed=1), 128
+    if name == "grid3d_64":
+        return gen.grid_nd((64, 64, 64), "7"), 256
+    raise SystemExit("unknown workload " + name)
+
+
+def read_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def read_traffic(workload):
+    """dram bytes per traversal launch from the committed ncu summary."""
+    p = os.path.join(ROOT, "profiles", "traverse_%s.md" % workload)
+    if not os.path.exists(p):
+        return None
+    for line in open(p):
+        if line.startswith("dram_bytes_per_launch:"):
+            try:
+                return float(line.split(":", 1)[1].strip().split()[0])
+            except ValueError:
+                return None
+    return None
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle samples during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), "--query-gpu=" + self.FIELDS,
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx.append(float(parts[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": float(max(mx)),
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def cpu_sample(rp, col, seconds, seed=0):
+    """Oracle (label search, all host threads) on random source rows of the
+    same matrix until `seconds` of work; returns GTEPS over the sample."""
+    from oracle import oracle as O
+    from gsofatpds_b200 import gen
+    beg, end = gen.csr_to_beg_end(rp)
+    n = beg.shape[0]
+    rng = np.random.default_rng(seed)
+    perm = rng.permutation(n).astype(np.int32)
+    done = 0
+    edges = 0
+    t0 = time.perf_counter()
+    batch = 64
+    while done < n and time.perf_counter() - t0 < seconds:
+        rows = np.sort(perm[done:done + batch])
+        r = O.rows(beg, end, col, rows=rows)
+        edges += int(r["e_alg"].sum())
+        done += rows.shape[0]
+        batch = min(batch * 2, 4096)
+    dt = time.perf_counter() - t0
+    cores = os.cpu_count() or 1
+    return dict(value=edges / dt / 1e9, unit="GTEPS", cores=cores, kind="port",
+                sample="%d random source rows of %d (%.1f%%), %.3g edges_alg, %.1f s" %
+                       (done, n, 100.0 * done / n, edges, dt))
+
+
+def run_reference(args, rank, world):
+    """Reference arm: the CPU restatement of the reference's traversal on the
+    host cores (the reference's own implementation of this path exists only
+    as CUDA kernels; its GPU build is not run here)."""
+    if rank != 0:
+        return
+    (n, rp, col), mss = make_workload(args.workload)
+    per_step = max(2.0, min(20.0, 60.0 / max(args.steps + args.warmup, 1)))
+    for i in range(args.warmup):
+        cpu_sample(rp, col, per_step / 2, seed=100 + i)
+    vals = []
+    last = None
+    for i in range(args.steps):
+        last = cpu_sample(rp, col, per_step, seed=i)
+        vals.append(last["value"])
+    v = float(np.median(vals))
+    cb = dict(last)
+    cb["value"] = v
+    line = {"impl": "reference", "metric": "fill_path_gteps", "value": v, "unit": "GTEPS",
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int32",
+            "data": "synthetic", "config": {"workload": WORKLOADS[args.workload], "mss": mss},
+            "cpu_baseline": cb,
+            "e2e": {"value": v, "unit": "GTEPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="circuit_like", choices=sorted(WORKLOADS))
+    ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--threads-per-source", type=int, default=0)
+    args = ap.parse_args()
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return
+
+    import torch
+    import torch.distributed as dist
+    from datetime import timedelta
+
+    torch.cuda.set_device(local)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600),
+                                device_id=torch.device("cuda", local))
+
+    from gsofatpds_b200 import Context
+
+    (n, rp, col), mss = make_workload(args.workload)
+    nnz = int(rp[-1])
+    ctx = Context(local)
+    stream = torch.cuda.Stream()  # events and the library share this stream
+    torch.cuda.set_stream(stream)
+    ctx.set_stream(stream.cuda_stream)
+    kw = dict(max_supernode_size=mss, threads_per_source=args.threads_per_source)
+
+    m = ctx.load_rowptr(rp, col)
+    # L2 flush buffer (> 126 MB L2) written between timed steps
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    for _ in range(args.warmup):
+        r = ctx.factor(m, **kw)
+        r.close()
+
+    # ---- device-resident timing
+    clocks = ClockSampler(local)
+    barrier()
+    clocks.start()
+    step_ms, trav_ms = [], []
+    counts = None
+    for _ in range(args.steps):
+        flush.zero_()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        r = ctx.factor(m, **kw)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        step_ms.append(e0.elapsed_time(e1))
+        trav_ms.append(r.counts["ms_traverse"])
+        counts = r.counts
+        r.close()
+    barrier()
+    clk = clocks.stop()
+    tot_ms = float(sum(step_ms))
+    t = torch.tensor([tot_ms], dtype=torch.float64, device="cuda")
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    max_ms = float(t.item())
+    edges = counts["edges_alg"]
+    value = world * args.steps * edges / (max_ms / 1e3) / 1e9
+
+    # ---- end to end through the C-ABI with host buffers
+    beg = torch.from_numpy(np.ascontiguousarray(rp[:-1])).pin_memory()
+    end = torch.from_numpy(np.ascontiguousarray(rp[1:])).pin_memory()
+    colp = torch.from_numpy(np.ascontiguousarray(col)).pin_memory()
+    out_u = torch.empty(n, dtype=torch.int32).pin_memory()
+    out_l = torch.empty(n, dtype=torch.int32).pin_memory()
+    out_z = torch.empty(n, dtype=torch.int32).pin_memory()
+    import ctypes
+    L = ctx._L
+    e2e_ms = []
+    barrier()
+    for _ in range(args.steps):
+        flush.zero_()
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        mh = ctypes.c_void_p()
+        ctx._check(L.gsofa_load_csr(ctx.handle, n, nnz, ctypes.c_void_p(beg.data_ptr()),
+                                    ctypes.c_void_p(end.data_ptr()), ctypes.c_void_p(colp.data_ptr()),
+                                    ctypes.byref(mh)), "load_csr")
+        o = ctx.opts(**kw)
+        rh = ctypes.c_void_p()
+        ctx._check(L.gsofa_factor_symbolic(ctx.handle, mh, ctypes.byref(o), ctypes.byref(rh)), "factor")
+        ctx._check(L.gsofa_result_row_counts(rh, ctypes.c_void_p(out_u.data_ptr()),
+                                             ctypes.c_void_p(out_z.data_ptr()),
+                                             ctypes.c_void_p(out_l.data_ptr()), None), "row_counts")
+        e1.record(stream)
+        torch.cuda.synchronize()
+        e2e_ms.append(e0.elapsed_time(e1))
+        L.gsofa_result_destroy(rh)
+        L.gsofa_matrix_destroy(mh)
+    barrier()
+    t = torch.tensor([float(sum(e2e_ms))], dtype=torch.float64, device="cuda")
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    e2e_value = world * args.steps * edges / (float(t.item()) / 1e3) / 1e9
+    h2d = (2 * n + nnz) * 4
+    d2h = 3 * n * 4
+
+    if rank == 0:
+        peak, peak_kind = read_peaks()
+        trav = float(np.mean(trav_ms))
+        w_out = 11 * n  # nnz_u, nz_row_u, nnz_lc, 2 digests (u64), 128-bit L-mask per row
+        bytes_alg = 8 * edges + 16 * counts["vertices_alg"] + 4 * w_out
+        achieved = bytes_alg / (trav / 1e3) / 1e9
+        traffic = read_traffic(args.workload)
+        roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak, "traffic": traffic,
+                "peak_kind": peak_kind + " (MEASURED_PEAKS hbm_gbs)",
+                "kernel": "traverse_kernel", "kernel_ms": trav,
+                "bytes_alg": bytes_alg}
+        line = {"metric": "fill_path_gteps", "value": value, "unit": "GTEPS", "n_gpus": world,
+                "steps": args.steps, "warmup": args.warmup,
+                "ms_per_step": max_ms / args.steps, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "int32", "data": "synthetic",
+                "config": {"workload": WORKLOADS[args.workload], "n": n, "nnz": nnz, "mss": mss,
+                           "l2": "flushed (256 MB write) before every timed step",
+                           "parallelism": "replicas" if world > 1 else "single"},
+                "ms_per_matrix": max_ms / args.steps, "matrices_per_s": world * args.steps / (max_ms / 1e3),
+                "fill_count": counts["fill_count"], "nnz_lu": counts["nnz_lu"],
+                "n_supernodes": counts["n_supernodes"], "edges_alg": edges,
+                "roofline": roof,
+                "e2e": {"value": e2e_value, "unit": "GTEPS", "h2d_bytes_per_step": h2d,
+                        "d2h_bytes_per_step": d2h, "ms_per_step": float(np.mean(e2e_ms))},
+                "clocks": clk,
+                "gpu_launches": 2 * args.steps}
+        if world == 1 and args.cpu_seconds > 0:
+            line["cpu_baseline"] = cpu_sample(rp, col, args.cpu_seconds)
+        print(json.dumps(line), flush=True)
+
+    m.close()
+    ctx.close()
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

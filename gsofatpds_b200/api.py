@@ -1,0 +1,226 @@
+"""Python host interface over the C-ABI (include/gsofa.h).
+
+Mirrors the reference's interface for the symbolic-factorization path:
+``symbfact_min_id(argv)`` takes the same argument vectors as the reference's
+``symbfact_min_id(argc, argv, rank, fill_count, time, N_supernodes, TEPS)``
+(gSoFa_SOAComparison/symbfact_warp_centric_new_scheduling.cuh:2529,
+SpaceOptimization/symbfact.cuh:1553) and returns the same four outputs, while
+``Context`` / ``Matrix`` / ``Result`` expose the handle-based calls for
+callers that keep matrices device-resident.  Errors raise ``GsofaError``
+carrying the library's status code; nothing here falls back to the CPU.
+"""
+import ctypes
+
+import numpy as np
+
+from . import _lib as C
+
+__all__ = ["GsofaError", "Context", "Matrix", "Result", "symbfact_min_id"]
+
+
+class GsofaError(RuntimeError):
+    def __init__(self, status, message):
+        super().__init__("%s (status %d)" % (message, status))
+        self.status = status
+
+
+def _ptr(a):
+    return None if a is None else a.ctypes.data_as(ctypes.c_void_p)
+
+
+class Context:
+    """One device context (memory budget, stream, workspace)."""
+
+    def __init__(self, device=0, budget_bytes=0):
+        self._L = C.load()
+        h = ctypes.c_void_p()
+        rc = self._L.gsofa_create(int(device), int(budget_bytes), ctypes.byref(h))
+        if rc != C.OK:
+            raise GsofaError(rc, "gsofa_create failed: %s" % self._L.gsofa_status_string(rc).decode())
+        self._h = h
+        self.device = device
+
+    def _check(self, rc, what):
+        if rc != C.OK:
+            msg = self._L.gsofa_last_error(self._h).decode(errors="replace")
+            raise GsofaError(rc, "%s: %s" % (what, msg))
+
+    @property
+    def handle(self):
+        return self._h
+
+    def set_stream(self, stream_ptr):
+        """Launch on this CUDA stream (an int cudaStream_t, e.g.
+        torch.cuda.current_stream().cuda_stream); None = own stream."""
+        self._check(self._L.gsofa_set_stream(self._h, ctypes.c_void_p(stream_ptr or 0)), "set_stream")
+
+    def memory_used(self):
+        v = ctypes.c_size_t()
+        self._check(self._L.gsofa_memory_used(self._h, ctypes.byref(v)), "memory_used")
+        return v.value
+
+    def load_csr(self, row_begin, row_end, col):
+        """Host arrays -> device-resident matrix.  Rows may be unsorted and
+        non-contiguous (row v is col[row_begin[v]:row_end[v]])."""
+        b = np.ascontiguousarray(row_begin, dtype=np.int32)
+        e = np.ascontiguousarray(row_end, dtype=np.int32)
+        c = np.ascontiguousarray(col, dtype=np.int32)
+        if b.shape != e.shape:
+            raise GsofaError(C.ERR_ARG, "row_begin and row_end differ in length")
+        h = ctypes.c_void_p()
+        self._check(self._L.gsofa_load_csr(self._h, b.shape[0], c.shape[0], _ptr(b), _ptr(e),
+                                           _ptr(c), ctypes.byref(h)), "load_csr")
+        return Matrix(self, h)
+
+    def load_rowptr(self, rowptr, col):
+        rowptr = np.ascontiguousarray(rowptr, dtype=np.int32)
+        return self.load_csr(rowptr[:-1], rowptr[1:], col)
+
+    def load_files(self, beg_file, end_file, csr_file):
+        h = ctypes.c_void_p()
+        self._check(self._L.gsofa_load_csr_files(self._h, beg_file.encode(), end_file.encode(),
+                                                 csr_file.encode(), ctypes.byref(h)), "load_files")
+        return Matrix(self, h)
+
+    @staticmethod
+    def opts(max_supernode_size=128, threads_per_source=0, sources_in_flight=0,
+             supernodes=True, digests=True, l_row_stats=False, pattern=False):
+        o = C.Opts()
+        o.max_supernode_size = int(max_supernode_size)
+        o.threads_per_source = int(threads_per_source)
+        o.sources_in_flight = int(sources_in_flight)
+        o.flags = ((C.SUPERNODES if supernodes else 0) | (C.DIGESTS if digests else 0) |
+                   (C.L_ROW_STATS if l_row_stats else 0) | (C.PATTERN if pattern else 0))
+        return o
+
+    def factor(self, mat, **kw):
+        o = self.opts(**kw)
+        h = ctypes.c_void_p()
+        self._check(self._L.gsofa_factor_symbolic(self._h, mat.handle, ctypes.byref(o),
+                                                  ctypes.byref(h)), "factor_symbolic")
+        return Result(self, h)
+
+    def factor_batch(self, mats, **kw):
+        o = self.opts(**kw)
+        k = len(mats)
+        arr = (ctypes.c_void_p * max(k, 1))(*[m.handle for m in mats])
+        outs = (ctypes.c_void_p * max(k, 1))()
+        self._check(self._L.gsofa_factor_batch(self._h, arr, k, ctypes.byref(o), outs),
+                    "factor_batch")
+        return [Result(self, ctypes.c_void_p(outs[i])) for i in range(k)]
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._L.gsofa_destroy(self._h)
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+
+class Matrix:
+    def __init__(self, ctx, h):
+        self.ctx = ctx
+        self._h = h
+        n = ctypes.c_int32()
+        nnz = ctypes.c_int64()
+        ctx._check(ctx._L.gsofa_matrix_info(h, ctypes.byref(n), ctypes.byref(nnz)), "matrix_info")
+        self.n = n.value
+        self.nnz = nnz.value
+
+    @property
+    def handle(self):
+        return self._h
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self.ctx._L.gsofa_matrix_destroy(self._h)
+            self._h = None
+
+
+class Result:
+    def __init__(self, ctx, h):
+        self.ctx = ctx
+        self._h = h
+        c = C.Counts()
+        ctx._check(ctx._L.gsofa_result_counts(h, ctypes.byref(c)), "result_counts")
+        self.counts = {f: getattr(c, f) for f, _ in C.Counts._fields_ if f != "reserved"}
+        self.n = c.n
+
+    def row_counts(self, l_rows=False):
+        n = self.n
+        u = np.zeros(n, np.int32)
+        nzu = np.zeros(n, np.int32)
+        lc = np.zeros(n, np.int32)
+        lr = np.zeros(n, np.int32) if l_rows else None
+        self.ctx._check(self.ctx._L.gsofa_result_row_counts(self._h, _ptr(u), _ptr(nzu), _ptr(lc),
+                                                            _ptr(lr)), "row_counts")
+        out = dict(nnz_u_row=u, nz_row_u=nzu, nnz_l_col=lc)
+        if l_rows:
+            out["nnz_l_row"] = lr
+        return out
+
+    def digests(self, l_rows=False):
+        n = self.n
+        du = np.zeros(n, np.uint64)
+        dl = np.zeros(n, np.uint64)
+        dr = np.zeros(n, np.uint64) if l_rows else None
+        self.ctx._check(self.ctx._L.gsofa_result_digests(self._h, _ptr(du), _ptr(dl), _ptr(dr)),
+                        "digests")
+        out = dict(dig_u_row=du, dig_l_col=dl)
+        if l_rows:
+            out["dig_l_row"] = dr
+        return out
+
+    def supernodes(self):
+        flags = np.zeros(self.n, np.int8)
+        cnt = ctypes.c_int64()
+        self.ctx._check(self.ctx._L.gsofa_result_supernodes(self._h, _ptr(flags), None, 0,
+                                                            ctypes.byref(cnt)), "supernodes")
+        return flags, np.nonzero(flags)[0].astype(np.int32)
+
+    def lmask(self):
+        m = np.zeros((self.n, 4), np.uint32)
+        self.ctx._check(self.ctx._L.gsofa_result_lmask(self._h, _ptr(m)), "lmask")
+        return m
+
+    def _pattern(self, fn):
+        ptr = np.zeros(self.n + 1, np.int64)
+        self.ctx._check(fn(self._h, _ptr(ptr), None, 0), "pattern")
+        ids = np.zeros(max(int(ptr[-1]), 1), np.int32)
+        self.ctx._check(fn(self._h, _ptr(ptr), _ptr(ids), ids.shape[0]), "pattern")
+        return ptr, ids[:ptr[-1]]
+
+    def pattern_u(self):
+        """U by rows: (rowptr[n+1], sorted column ids)."""
+        return self._pattern(self.ctx._L.gsofa_result_pattern_u)
+
+    def pattern_l(self):
+        """L by columns: (colptr[n+1], sorted row ids)."""
+        return self._pattern(self.ctx._L.gsofa_result_pattern_l)
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self.ctx._L.gsofa_result_destroy(self._h)
+            self._h = None
+
+
+def symbfact_min_id(argv, rank=0):
+    """The reference's entry point: argv is the full vector including the
+    program name (11 entries: SOA layout; 6 entries: SPO layout).
+    Returns (fill_count, time_ms, N_supernodes, TEPS_edges)."""
+    L = C.load()
+    args = [a.encode() if isinstance(a, str) else a for a in argv]
+    arr = (ctypes.c_char_p * len(args))(*args)
+    fill = ctypes.c_uint64()
+    ms = ctypes.c_double()
+    nsup = ctypes.c_int32()
+    teps = ctypes.c_uint64()
+    rc = L.gsofa_symbfact_min_id(len(args), arr, int(rank), ctypes.byref(fill), ctypes.byref(ms),
+                                 ctypes.byref(nsup), ctypes.byref(teps))
+    if rc != C.OK:
+        raise GsofaError(rc, "symbfact_min_id failed: %s" % L.gsofa_status_string(rc).decode())
+    return fill.value, ms.value, nsup.value, teps.value

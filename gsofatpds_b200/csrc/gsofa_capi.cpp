@@ -1,0 +1,932 @@
+// gsofa_capi.cpp -- host side of libgsofa.so: the C-ABI declared in
+// include/gsofa.h.  Owns device memory (a dedicated stream-ordered pool with
+// budget accounting), device-resident matrices and results, the launch
+// configuration of the traversal kernel, and the reference-shaped entry point.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cerrno>
+#include <chrono>
+#include <cstdarg>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <memory>
+#include <mutex>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "../../include/gsofa.h"
+#include "gsofa_internal.h"
+
+using namespace gsofa;
+
+struct gsofa_ctx {
+    int device = 0;
+    int sm_count = 0;
+    int smem_optin = 0;
+    size_t budget = 0;
+    size_t used = 0;
+    cudaStream_t own_stream = nullptr;
+    cudaStream_t stream = nullptr;
+    cudaMemPool_t pool = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr, evt = nullptr;
+    std::recursive_mutex mu;
+    std::string err;
+    // pinned staging
+    unsigned long long* h_counters = nullptr;  // CNT_SLOTS
+    int32_t* h_status = nullptr;
+    // grown workspace
+    void* queue = nullptr;
+    size_t queue_bytes = 0;
+    void* gbitmap = nullptr;
+    size_t gbitmap_bytes = 0;
+    void* small = nullptr;  // work counter (8 B) + status (4 B)
+    void* scan_tmp = nullptr;
+    size_t scan_tmp_bytes = 0;
+};
+
+struct gsofa_matrix {
+    gsofa_ctx* ctx = nullptr;
+    int32_t n = 0;
+    int64_t nnz = 0;
+    int32_t* rowptr = nullptr;
+    int32_t* col = nullptr;
+    int32_t* trowptr = nullptr;
+    int32_t* tcol = nullptr;
+    size_t bytes = 0;
+};
+
+struct gsofa_result {
+    gsofa_ctx* ctx = nullptr;
+    int32_t n = 0;
+    uint32_t flags = 0;
+    int32_t mss = 128;
+    void* arena = nullptr;  // one device block holding every array below
+    size_t bytes = 0;
+    int32_t* nnz_u = nullptr;
+    int32_t* nz_row_u = nullptr;
+    uint64_t* dig_u = nullptr;
+    int32_t* nnz_lc = nullptr;
+    uint64_t* dig_lc = nullptr;
+    uint32_t* lmask = nullptr;
+    int32_t* nnz_lr = nullptr;
+    uint64_t* dig_lr = nullptr;
+    int8_t* sflags = nullptr;
+    unsigned long long* counters = nullptr;
+    // pattern (separate allocation, only with GSOFA_PATTERN)
+    void* parena = nullptr;
+    size_t pbytes = 0;
+    int64_t* uptr = nullptr;
+    int32_t* ucols = nullptr;
+    int64_t* lptr = nullptr;
+    int32_t* lrows = nullptr;
+    gsofa_counts counts{};
+};
+
+// ---------------------------------------------------------------------------
+namespace {
+
+int set_err(gsofa_ctx* ctx, int status, const char* fmt, ...) {
+    if (ctx) {
+        char buf[512];
+        va_list ap;
+        va_start(ap, fmt);
+        vsnprintf(buf, sizeof(buf), fmt, ap);
+        va_end(ap);
+        ctx->err = buf;
+    }
+    return status;
+}
+
+int cuda_fail(gsofa_ctx* ctx, cudaError_t e, const char* where) {
+    return set_err(ctx, GSOFA_ERR_CUDA, "%s: %s", where, cudaGetErrorString(e));
+}
+
+#define CK(call)                                          \
+    do {                                                  \
+        cudaError_t e_ = (call);                          \
+        if (e_ != cudaSuccess) return cuda_fail(ctx, e_, #call); \
+    } while (0)
+
+int dev_alloc(gsofa_ctx* ctx, size_t bytes, void** p) {
+    *p = nullptr;
+    if (bytes == 0) return GSOFA_OK;
+    bytes = (bytes + 255) & ~(size_t)255;
+    if (ctx->used + bytes > ctx->budget)
+        return set_err(ctx, GSOFA_ERR_OOM_BUDGET,
+                       "allocation of %zu bytes exceeds the budget (%zu of %zu bytes in use)",
+                       bytes, ctx->used, ctx->budget);
+    cudaError_t e = cudaMallocFromPoolAsync(p, bytes, ctx->pool, ctx->stream);
+    if (e != cudaSuccess) {
+        *p = nullptr;
+        return cuda_fail(ctx, e, "cudaMallocFromPoolAsync");
+    }
+    ctx->used += bytes;
+    return GSOFA_OK;
+}
+
+void dev_free(gsofa_ctx* ctx, void* p, size_t bytes) {
+    if (!p) return;
+    bytes = (bytes + 255) & ~(size_t)255;
+    cudaFreeAsync(p, ctx->stream);
+    ctx->used -= std::min(ctx->used, bytes);
+}
+
+// Grow-only workspace buffer.
+int ensure(gsofa_ctx* ctx, void** p, size_t* have, size_t need) {
+    if (*have >= need) return GSOFA_OK;
+    dev_free(ctx, *p, *have);
+    *p = nullptr;
+    *have = 0;
+    int rc = dev_alloc(ctx, need, p);
+    if (rc) return rc;
+    *have = (need + 255) & ~(size_t)255;
+    return GSOFA_OK;
+}
+
+size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
+
+long long bitmap_words(int32_t n) { return (((long long)n + 31) >> 5) + 6; }
+
+int default_block(int32_t nmax) {
+    // Measured-on-B200 defaults are refined by the Python autotuner; these
+    // are the starting points: small orders have short searches.
+    if (nmax < 8192) return 256;
+    return 512;
+}
+
+struct LaunchCfg {
+    int block = 512;
+    int grid = 0;
+    bool smem_bitmap = true;
+    size_t smem = 0;
+    long long words = 0;
+};
+
+int plan_launch(gsofa_ctx* ctx, int32_t nmax, const gsofa_opts* o, LaunchCfg* c) {
+    c->block = o->threads_per_source > 0 ? o->threads_per_source : default_block(nmax);
+    if (c->block != 128 && c->block != 256 && c->block != 512 && c->block != 1024)
+        return set_err(ctx, GSOFA_ERR_ARG, "threads_per_source must be 128, 256, 512 or 1024");
+    c->words = bitmap_words(nmax);
+    size_t bytes = (size_t)c->words * 4;
+    bytes = (bytes + 15) & ~(size_t)15;
+    // leave room for the kernel's static shared memory (reduction + scan)
+    c->smem_bitmap = bytes + 12 * 1024 <= (size_t)ctx->smem_optin &&
+                     !(o->flags & GSOFA_FORCE_GLOBAL_BITMAP);
+    c->smem = c->smem_bitmap ? bytes : 0;
+    int occ = traverse_occupancy(c->block, c->smem_bitmap, c->smem);
+    if (occ <= 0)
+        return set_err(ctx, GSOFA_ERR_UNSUPPORTED,
+                       "traversal kernel cannot be resident (block %d, %zu B shared)", c->block,
+                       c->smem);
+    c->grid = occ * ctx->sm_count;
+    if (o->sources_in_flight > 0) c->grid = std::min(c->grid, o->sources_in_flight);
+    return GSOFA_OK;
+}
+
+int check_status(gsofa_ctx* ctx) {
+    int32_t s = *ctx->h_status;
+    if (s & DEV_ERR_COL_RANGE) return set_err(ctx, GSOFA_ERR_ARG, "column id outside [0, n)");
+    if (s & DEV_ERR_ROW_RANGE) return set_err(ctx, GSOFA_ERR_ARG, "row interval outside [0, nnz)");
+    if (s & DEV_ERR_QUEUE) return set_err(ctx, GSOFA_ERR_OVERFLOW, "traversal queue bound exceeded");
+    return GSOFA_OK;
+}
+
+int32_t* work_counter_status(gsofa_ctx* ctx, unsigned long long** wc) {
+    *wc = reinterpret_cast<unsigned long long*>(ctx->small);
+    return reinterpret_cast<int32_t*>(reinterpret_cast<char*>(ctx->small) + 64);
+}
+
+void result_free(gsofa_result* r) {
+    if (!r) return;
+    if (r->ctx) {
+        std::lock_guard<std::recursive_mutex> g(r->ctx->mu);
+        dev_free(r->ctx, r->arena, r->bytes);
+        dev_free(r->ctx, r->parena, r->pbytes);
+    }
+    delete r;
+}
+
+// Carve the per-row result arrays out of one arena.
+int result_alloc(gsofa_ctx* ctx, int32_t n, uint32_t flags, int32_t mss, gsofa_result** out) {
+    gsofa_result* r = new (std::nothrow) gsofa_result();
+    if (!r) return set_err(ctx, GSOFA_ERR_OOM_BUDGET, "host allocation failed");
+    r->ctx = ctx;
+    r->n = n;
+    r->flags = flags;
+    r->mss = mss;
+    const size_t N = (size_t)std::max(n, 1);
+    const bool dig = flags & GSOFA_DIGESTS;
+    const bool lrow = flags & GSOFA_L_ROW_STATS;
+    size_t off[12], sz[12];
+    sz[0] = 4 * N;                       // nnz_u
+    sz[1] = 4 * N;                       // nz_row_u
+    sz[2] = dig ? 8 * N : 0;             // dig_u
+    sz[3] = 4 * N;                       // nnz_lc
+    sz[4] = dig ? 8 * N : 0;             // dig_lc
+    sz[5] = 16 * N;                      // lmask
+    sz[6] = lrow ? 4 * N : 0;            // nnz_lr
+    sz[7] = lrow ? 8 * N : 0;            // dig_lr
+    sz[8] = N;                           // supernode flags
+    sz[9] = 8 * CNT_SLOTS;               // counters
+    size_t total = 0;
+    for (int i = 0; i < 10; i++) {
+        off[i] = total;
+        total += align256(sz[i]);
+    }
+    int rc = dev_alloc(ctx, total, &r->arena);
+    if (rc) {
+        delete r;
+        return rc;
+    }
+    r->bytes = total;
+    char* b = reinterpret_cast<char*>(r->arena);
+    r->nnz_u = reinterpret_cast<int32_t*>(b + off[0]);
+    r->nz_row_u = reinterpret_cast<int32_t*>(b + off[1]);
+    r->dig_u = dig ? reinterpret_cast<uint64_t*>(b + off[2]) : nullptr;
+    r->nnz_lc = reinterpret_cast<int32_t*>(b + off[3]);
+    r->dig_lc = dig ? reinterpret_cast<uint64_t*>(b + off[4]) : nullptr;
+    r->lmask = reinterpret_cast<uint32_t*>(b + off[5]);
+    r->nnz_lr = lrow ? reinterpret_cast<int32_t*>(b + off[6]) : nullptr;
+    r->dig_lr = lrow ? reinterpret_cast<uint64_t*>(b + off[7]) : nullptr;
+    r->sflags = reinterpret_cast<int8_t*>(b + off[8]);
+    r->counters = reinterpret_cast<unsigned long long*>(b + off[9]);
+    // zero the scatter targets, the counters and the flags
+    cudaError_t e = cudaSuccess;
+    if (lrow) {
+        e = cudaMemsetAsync(r->nnz_lr, 0, 4 * N, ctx->stream);
+        if (e == cudaSuccess) e = cudaMemsetAsync(r->dig_lr, 0, 8 * N, ctx->stream);
+    }
+    if (e == cudaSuccess) e = cudaMemsetAsync(r->counters, 0, 8 * CNT_SLOTS, ctx->stream);
+    if (e == cudaSuccess) e = cudaMemsetAsync(r->sflags, 0, N, ctx->stream);
+    if (e != cudaSuccess) {
+        result_free(r);
+        return cuda_fail(ctx, e, "result init");
+    }
+    *out = r;
+    return GSOFA_OK;
+}
+
+MatDesc make_desc(const gsofa_matrix* m, const gsofa_result* r, long long base) {
+    MatDesc d{};
+    d.n = m->n;
+    d.flags = (int32_t)r->flags;
+    d.rowptr = m->rowptr;
+    d.col = m->col;
+    d.trowptr = m->trowptr;
+    d.tcol = m->tcol;
+    d.nnz_u = r->nnz_u;
+    d.nz_row_u = r->nz_row_u;
+    d.dig_u = r->dig_u;
+    d.nnz_lc = r->nnz_lc;
+    d.dig_lc = r->dig_lc;
+    d.lmask = r->lmask;
+    d.nnz_lr = r->nnz_lr;
+    d.dig_lr = r->dig_lr;
+    d.counters = r->counters;
+    d.uptr = r->uptr;
+    d.ucols = r->ucols;
+    d.lptr = r->lptr;
+    d.lrows = r->lrows;
+    d.item_base = base;
+    return d;
+}
+
+// Runs the traversal (and optionally supernodes / pattern) for `count`
+// matrices in one persistent launch.  results[i] must be freshly allocated.
+int run_factor(gsofa_ctx* ctx, const gsofa_matrix* const* mats, int32_t count,
+               const gsofa_opts* o, gsofa_result** res) {
+    int32_t nmax = 0;
+    long long items = 0;
+    for (int32_t i = 0; i < count; i++) {
+        nmax = std::max(nmax, mats[i]->n);
+        items += 2ll * mats[i]->n;
+    }
+    LaunchCfg cfg;
+    int rc = plan_launch(ctx, std::max(nmax, 1), o, &cfg);
+    if (rc) return rc;
+    rc = ensure(ctx, &ctx->queue, &ctx->queue_bytes, (size_t)cfg.grid * (size_t)std::max(nmax, 1) * 4);
+    if (rc) return rc;
+    if (!cfg.smem_bitmap) {
+        rc = ensure(ctx, &ctx->gbitmap, &ctx->gbitmap_bytes, (size_t)cfg.grid * (size_t)cfg.words * 4);
+        if (rc) return rc;
+    }
+    // matrix descriptors
+    std::vector<MatDesc> descs((size_t)count);
+    long long base = 0;
+    for (int32_t i = 0; i < count; i++) {
+        descs[i] = make_desc(mats[i], res[i], base);
+        base += 2ll * mats[i]->n;
+    }
+    void* ddesc = nullptr;
+    rc = dev_alloc(ctx, sizeof(MatDesc) * (size_t)count, &ddesc);
+    if (rc) return rc;
+    CK(cudaMemcpyAsync(ddesc, descs.data(), sizeof(MatDesc) * (size_t)count, cudaMemcpyHostToDevice,
+                       ctx->stream));
+    unsigned long long* wc = nullptr;
+    int32_t* dstatus = work_counter_status(ctx, &wc);
+    CK(cudaMemsetAsync(ctx->small, 0, 128, ctx->stream));
+
+    TraverseLaunch L{};
+    L.mats = reinterpret_cast<const MatDesc*>(ddesc);
+    L.nmats = count;
+    L.total_items = items;
+    L.work_counter = wc;
+    L.queue = reinterpret_cast<int32_t*>(ctx->queue);
+    L.queue_stride = std::max(nmax, 1);
+    L.gbitmap = reinterpret_cast<uint32_t*>(ctx->gbitmap);
+    L.bitmap_words = cfg.words;
+    L.status = dstatus;
+    L.pattern_pass = 0;
+
+    CK(cudaEventRecord(ctx->ev0, ctx->stream));
+    if (items > 0) CK(launch_traverse(L, cfg.block, cfg.grid, cfg.smem_bitmap, cfg.smem, ctx->stream));
+    CK(cudaEventRecord(ctx->evt, ctx->stream));
+    for (int32_t i = 0; i < count; i++) {
+        if ((o->flags & GSOFA_SUPERNODES) && mats[i]->n > 0)
+            CK(launch_supernodes(mats[i]->n, o->max_supernode_size, res[i]->nz_row_u, res[i]->lmask,
+                                 res[i]->sflags, res[i]->counters, ctx->stream));
+    }
+    CK(cudaEventRecord(ctx->ev1, ctx->stream));
+    CK(cudaMemcpyAsync(ctx->h_status, dstatus, 4, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    rc = check_status(ctx);
+    if (rc) {
+        dev_free(ctx, ddesc, sizeof(MatDesc) * (size_t)count);
+        return rc;
+    }
+    float ms = 0.f, ms_trav = 0.f;
+    CK(cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
+    CK(cudaEventElapsedTime(&ms_trav, ctx->ev0, ctx->evt));
+
+    // pattern pass (second traversal writing sorted ids)
+    if (o->flags & GSOFA_PATTERN) {
+        for (int32_t i = 0; i < count; i++) {
+            gsofa_result* r = res[i];
+            CK(cudaMemcpyAsync(ctx->h_counters, r->counters, 8 * CNT_SLOTS, cudaMemcpyDeviceToHost,
+                               ctx->stream));
+            CK(cudaStreamSynchronize(ctx->stream));
+            const size_t N = (size_t)r->n + 1;
+            const size_t nu = ctx->h_counters[CNT_NNZ_U], nl = ctx->h_counters[CNT_NNZ_L];
+            size_t total = align256(8 * N) * 2 + align256(4 * std::max<size_t>(nu, 1)) +
+                           align256(4 * std::max<size_t>(nl, 1));
+            rc = dev_alloc(ctx, total, &r->parena);
+            if (rc) return rc;
+            r->pbytes = total;
+            char* b = reinterpret_cast<char*>(r->parena);
+            r->uptr = reinterpret_cast<int64_t*>(b);
+            r->lptr = reinterpret_cast<int64_t*>(b + align256(8 * N));
+            r->ucols = reinterpret_cast<int32_t*>(b + 2 * align256(8 * N));
+            r->lrows = reinterpret_cast<int32_t*>(b + 2 * align256(8 * N) +
+                                                  align256(4 * std::max<size_t>(nu, 1)));
+            rc = ensure(ctx, &ctx->scan_tmp, &ctx->scan_tmp_bytes, pattern_scan_bytes(r->n));
+            if (rc) return rc;
+            CK(launch_pattern_ptrs(r->n, r->nnz_u, r->nnz_lc, r->uptr, r->lptr, ctx->scan_tmp,
+                                   ctx->scan_tmp_bytes, ctx->stream));
+            descs[i] = make_desc(mats[i], r, descs[i].item_base);
+        }
+        CK(cudaMemcpyAsync(ddesc, descs.data(), sizeof(MatDesc) * (size_t)count,
+                           cudaMemcpyHostToDevice, ctx->stream));
+        CK(cudaMemsetAsync(ctx->small, 0, 128, ctx->stream));
+        L.pattern_pass = 1;
+        if (items > 0)
+            CK(launch_traverse(L, cfg.block, cfg.grid, cfg.smem_bitmap, cfg.smem, ctx->stream));
+        CK(cudaMemcpyAsync(ctx->h_status, dstatus, 4, cudaMemcpyDeviceToHost, ctx->stream));
+        CK(cudaStreamSynchronize(ctx->stream));
+        rc = check_status(ctx);
+        if (rc) {
+            dev_free(ctx, ddesc, sizeof(MatDesc) * (size_t)count);
+            return rc;
+        }
+    }
+    dev_free(ctx, ddesc, sizeof(MatDesc) * (size_t)count);
+
+    for (int32_t i = 0; i < count; i++) {
+        gsofa_result* r = res[i];
+        CK(cudaMemcpyAsync(ctx->h_counters, r->counters, 8 * CNT_SLOTS, cudaMemcpyDeviceToHost,
+                           ctx->stream));
+        CK(cudaStreamSynchronize(ctx->stream));
+        const unsigned long long* c = ctx->h_counters;
+        gsofa_counts& k = r->counts;
+        k.n = r->n;
+        k.fill_count = c[CNT_FILLS];
+        k.nnz_l = c[CNT_NNZ_L];
+        k.nnz_u = c[CNT_NNZ_U];
+        k.nnz_lu = c[CNT_NNZ_L] + c[CNT_NNZ_U] + (uint64_t)r->n;
+        k.n_supernodes = (o->flags & GSOFA_SUPERNODES) ? (int64_t)c[CNT_NSUP] + 1 : -1;
+        k.edges_alg = c[CNT_EDGES_ALG];
+        k.vertices_alg = c[CNT_VERTS_ALG];
+        k.edges_traversed = c[CNT_EDGES_TRAV];
+        k.ms_device = (double)ms;  // for a batch: the whole launch
+        k.ms_traverse = (double)ms_trav;
+    }
+    return GSOFA_OK;
+}
+
+int validate_opts(gsofa_ctx* ctx, const gsofa_opts* o) {
+    if (o->max_supernode_size <= 0)
+        return set_err(ctx, GSOFA_ERR_ARG, "max_supernode_size must be positive");
+    if (o->threads_per_source < 0 || o->sources_in_flight < 0)
+        return set_err(ctx, GSOFA_ERR_ARG, "negative launch option");
+    return GSOFA_OK;
+}
+
+// ---- fast ASCII reader --------------------------------------------------------
+int read_file(const char* path, std::string* out) {
+    FILE* f = fopen(path, "rb");
+    if (!f) return -1;
+    if (fseek(f, 0, SEEK_END) != 0) { fclose(f); return -1; }
+    long sz = ftell(f);
+    if (sz < 0) { fclose(f); return -1; }
+    rewind(f);
+    out->resize((size_t)sz);
+    size_t got = sz ? fread(&(*out)[0], 1, (size_t)sz, f) : 0;
+    fclose(f);
+    return got == (size_t)sz ? 0 : -1;
+}
+
+// Parses up to `count` whitespace-separated integers; returns how many.
+int64_t parse_ints(const std::string& s, size_t* pos, int64_t count, int32_t* out, bool* bad) {
+    const char* p = s.data() + *pos;
+    const char* e = s.data() + s.size();
+    int64_t i = 0;
+    while (i < count) {
+        while (p < e && (*p == ' ' || *p == '\n' || *p == '\r' || *p == '\t')) p++;
+        if (p >= e) break;
+        bool neg = false;
+        if (*p == '-') { neg = true; p++; }
+        if (p >= e || *p < '0' || *p > '9') { *bad = true; break; }
+        int64_t v = 0;
+        while (p < e && *p >= '0' && *p <= '9') { v = v * 10 + (*p - '0'); p++; if (v > 4294967295ll) { *bad = true; break; } }
+        out[i++] = (int32_t)(neg ? -v : v);
+    }
+    *pos = (size_t)(p - s.data());
+    return i;
+}
+
+}  // namespace
+
+// ============================================================================
+extern "C" {
+
+const char* gsofa_status_string(int s) {
+    switch (s) {
+        case GSOFA_OK: return "ok";
+        case GSOFA_ERR_ARG: return "invalid argument";
+        case GSOFA_ERR_IO: return "i/o error";
+        case GSOFA_ERR_OOM_BUDGET: return "memory budget exceeded";
+        case GSOFA_ERR_TIMEOUT: return "device wait timed out";
+        case GSOFA_ERR_OVERFLOW: return "queue bound exceeded";
+        case GSOFA_ERR_CUDA: return "cuda error";
+        case GSOFA_ERR_UNSUPPORTED: return "unsupported size or option";
+        case GSOFA_ERR_BUSY: return "busy";
+        default: return "unknown status";
+    }
+}
+
+int gsofa_opts_default(gsofa_opts* o) {
+    if (!o) return GSOFA_ERR_ARG;
+    o->max_supernode_size = 128;
+    o->threads_per_source = 0;
+    o->sources_in_flight = 0;
+    o->flags = GSOFA_SUPERNODES | GSOFA_DIGESTS;
+    return GSOFA_OK;
+}
+
+int gsofa_create(int device, size_t budget_bytes, gsofa_ctx** out) {
+    if (!out) return GSOFA_ERR_ARG;
+    *out = nullptr;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= 0) {
+        cudaGetLastError();
+        return GSOFA_ERR_CUDA;
+    }
+    if (device < 0 || device >= ndev) return GSOFA_ERR_ARG;
+    gsofa_ctx* ctx = new (std::nothrow) gsofa_ctx();
+    if (!ctx) return GSOFA_ERR_OOM_BUDGET;
+    ctx->device = device;
+    auto fail = [&](cudaError_t e) {
+        (void)e;
+        if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
+        if (ctx->ev0) cudaEventDestroy(ctx->ev0);
+        if (ctx->ev1) cudaEventDestroy(ctx->ev1);
+        if (ctx->evt) cudaEventDestroy(ctx->evt);
+        if (ctx->h_counters) cudaFreeHost(ctx->h_counters);
+        if (ctx->h_status) cudaFreeHost(ctx->h_status);
+        if (ctx->pool) cudaMemPoolDestroy(ctx->pool);
+        delete ctx;
+        return GSOFA_ERR_CUDA;
+    };
+    cudaError_t e = cudaSetDevice(device);
+    if (e != cudaSuccess) return fail(e);
+    cudaDeviceGetAttribute(&ctx->sm_count, cudaDevAttrMultiProcessorCount, device);
+    cudaDeviceGetAttribute(&ctx->smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device);
+    size_t fr = 0, tot = 0;
+    if ((e = cudaMemGetInfo(&fr, &tot)) != cudaSuccess) return fail(e);
+    ctx->budget = budget_bytes ? budget_bytes : (size_t)(0.9 * (double)fr);
+    if ((e = cudaStreamCreateWithFlags(&ctx->own_stream, cudaStreamNonBlocking)) != cudaSuccess)
+        return fail(e);
+    ctx->stream = ctx->own_stream;
+    if ((e = cudaEventCreate(&ctx->ev0)) != cudaSuccess) return fail(e);
+    if ((e = cudaEventCreate(&ctx->ev1)) != cudaSuccess) return fail(e);
+    if ((e = cudaEventCreate(&ctx->evt)) != cudaSuccess) return fail(e);
+    if ((e = cudaMallocHost((void**)&ctx->h_counters, 8 * CNT_SLOTS)) != cudaSuccess) return fail(e);
+    if ((e = cudaMallocHost((void**)&ctx->h_status, 64)) != cudaSuccess) return fail(e);
+    cudaMemPoolProps props{};
+    props.allocType = cudaMemAllocationTypePinned;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = device;
+    if ((e = cudaMemPoolCreate(&ctx->pool, &props)) != cudaSuccess) return fail(e);
+    uint64_t thr = UINT64_MAX;
+    cudaMemPoolSetAttribute(ctx->pool, cudaMemPoolAttrReleaseThreshold, &thr);
+    if (dev_alloc(ctx, 256, &ctx->small) != GSOFA_OK) return fail(cudaErrorMemoryAllocation);
+    *out = ctx;
+    return GSOFA_OK;
+}
+
+int gsofa_destroy(gsofa_ctx* ctx) {
+    if (!ctx) return GSOFA_ERR_ARG;
+    {
+        std::lock_guard<std::recursive_mutex> g(ctx->mu);
+        cudaSetDevice(ctx->device);
+        dev_free(ctx, ctx->queue, ctx->queue_bytes);
+        dev_free(ctx, ctx->gbitmap, ctx->gbitmap_bytes);
+        dev_free(ctx, ctx->scan_tmp, ctx->scan_tmp_bytes);
+        dev_free(ctx, ctx->small, 256);
+        cudaStreamSynchronize(ctx->stream);
+        cudaStreamSynchronize(ctx->own_stream);
+        cudaStreamDestroy(ctx->own_stream);
+        cudaEventDestroy(ctx->ev0);
+        cudaEventDestroy(ctx->ev1);
+        cudaEventDestroy(ctx->evt);
+        cudaFreeHost(ctx->h_counters);
+        cudaFreeHost(ctx->h_status);
+        cudaMemPoolDestroy(ctx->pool);
+    }
+    delete ctx;
+    return GSOFA_OK;
+}
+
+const char* gsofa_last_error(const gsofa_ctx* ctx) {
+    if (!ctx) return "null context";
+    return ctx->err.c_str();
+}
+
+int gsofa_set_stream(gsofa_ctx* ctx, void* s) {
+    if (!ctx) return GSOFA_ERR_ARG;
+    std::lock_guard<std::recursive_mutex> g(ctx->mu);
+    // drain work queued on the previous stream before switching
+    cudaStreamSynchronize(ctx->stream);
+    ctx->stream = s ? reinterpret_cast<cudaStream_t>(s) : ctx->own_stream;
+    return GSOFA_OK;
+}
+
+int gsofa_memory_used(const gsofa_ctx* ctx, size_t* bytes) {
+    if (!ctx || !bytes) return GSOFA_ERR_ARG;
+    *bytes = ctx->used;
+    return GSOFA_OK;
+}
+
+int gsofa_load_csr(gsofa_ctx* ctx, int32_t n, int64_t nnz, const int32_t* row_begin,
+                   const int32_t* row_end, const int32_t* col, gsofa_matrix** out) {
+    if (!ctx || !out) return GSOFA_ERR_ARG;
+    *out = nullptr;
+    std::lock_guard<std::recursive_mutex> g(ctx->mu);
+    if (n < 0 || nnz < 0) return set_err(ctx, GSOFA_ERR_ARG, "negative n or nnz");
+    if (n > 0 && (!row_begin || !row_end)) return set_err(ctx, GSOFA_ERR_ARG, "null row arrays");
+    if (nnz > 0 && !col) return set_err(ctx, GSOFA_ERR_ARG, "null column array");
+    if (nnz > INT32_MAX) return set_err(ctx, GSOFA_ERR_UNSUPPORTED, "nnz above 2^31-1");
+    if (cudaSetDevice(ctx->device) != cudaSuccess) return set_err(ctx, GSOFA_ERR_CUDA, "cudaSetDevice");
+    // host: row pointers of the packed layout, and a contiguity test
+    std::vector<int32_t> rowptr((size_t)n + 1);
+    int64_t acc = 0;
+    bool contiguous = true;
+    for (int32_t v = 0; v < n; v++) {
+        const int64_t b = row_begin[v], e = row_end[v];
+        if (b < 0 || e < b || e > nnz)
+            return set_err(ctx, GSOFA_ERR_ARG, "row %d interval [%lld,%lld) outside [0,%lld)", v,
+                           (long long)b, (long long)e, (long long)nnz);
+        if (b != acc) contiguous = false;
+        rowptr[v] = (int32_t)acc;
+        acc += e - b;
+        if (acc > INT32_MAX) return set_err(ctx, GSOFA_ERR_UNSUPPORTED, "packed nnz above 2^31-1");
+    }
+    rowptr[(size_t)n] = (int32_t)acc;
+    const int64_t packed = acc;
+
+    gsofa_matrix* m = new (std::nothrow) gsofa_matrix();
+    if (!m) return set_err(ctx, GSOFA_ERR_OOM_BUDGET, "host allocation failed");
+    m->ctx = ctx;
+    m->n = n;
+    m->nnz = packed;
+    const size_t N1 = (size_t)n + 1;
+    const size_t P = (size_t)std::max<int64_t>(packed, 1);
+    size_t total = align256(4 * N1) * 2 + align256(4 * P) * 2;
+    void* blk = nullptr;
+    int rc = dev_alloc(ctx, total, &blk);
+    if (rc) { delete m; return rc; }
+    m->bytes = total;
+    char* b = reinterpret_cast<char*>(blk);
+    m->rowptr = reinterpret_cast<int32_t*>(b);
+    m->trowptr = reinterpret_cast<int32_t*>(b + align256(4 * N1));
+    m->col = reinterpret_cast<int32_t*>(b + 2 * align256(4 * N1));
+    m->tcol = reinterpret_cast<int32_t*>(b + 2 * align256(4 * N1) + align256(4 * P));
+
+    // staging: raw input (beg, col_in) + transpose counters
+    const size_t Nin = (size_t)std::max<int64_t>(nnz, 1);
+    size_t scan_bytes = canonicalize_scan_bytes(n);
+    size_t stage = align256(4 * N1) + (contiguous ? 0 : align256(4 * Nin)) + align256(4 * N1) * 2 +
+                   align256(scan_bytes) + 256;
+    void* sblk = nullptr;
+    rc = dev_alloc(ctx, stage, &sblk);
+    if (rc) { dev_free(ctx, blk, total); delete m; return rc; }
+    char* s = reinterpret_cast<char*>(sblk);
+    int32_t* dbeg = reinterpret_cast<int32_t*>(s);
+    s += align256(4 * N1);
+    int32_t* dcol_in = m->col;
+    if (!contiguous) {
+        dcol_in = reinterpret_cast<int32_t*>(s);
+        s += align256(4 * Nin);
+    }
+    int32_t* tcount = reinterpret_cast<int32_t*>(s);
+    s += align256(4 * N1);
+    int32_t* tfill = reinterpret_cast<int32_t*>(s);
+    s += align256(4 * N1);
+    void* scan_tmp = s;
+
+    unsigned long long* wc = nullptr;
+    int32_t* dstatus = work_counter_status(ctx, &wc);
+    cudaError_t e = cudaSuccess;
+    auto cleanup = [&]() {
+        dev_free(ctx, sblk, stage);
+        dev_free(ctx, blk, total);
+        delete m;
+    };
+#define CKL(call)                                        \
+    do {                                                 \
+        e = (call);                                      \
+        if (e != cudaSuccess) { cleanup(); return cuda_fail(ctx, e, #call); } \
+    } while (0)
+    CKL(cudaMemsetAsync(ctx->small, 0, 128, ctx->stream));
+    if (n > 0) {
+        CKL(cudaMemcpyAsync(dbeg, contiguous ? rowptr.data() : row_begin, 4 * (size_t)n,
+                            cudaMemcpyHostToDevice, ctx->stream));
+        CKL(cudaMemcpyAsync(m->rowptr, rowptr.data(), 4 * N1, cudaMemcpyHostToDevice, ctx->stream));
+    } else {
+        CKL(cudaMemsetAsync(m->rowptr, 0, 4, ctx->stream));
+        CKL(cudaMemsetAsync(m->trowptr, 0, 4, ctx->stream));
+    }
+    if (contiguous) {
+        if (packed > 0)
+            CKL(cudaMemcpyAsync(m->col, col, 4 * (size_t)packed, cudaMemcpyHostToDevice, ctx->stream));
+    } else if (nnz > 0) {
+        CKL(cudaMemcpyAsync(dcol_in, col, 4 * (size_t)nnz, cudaMemcpyHostToDevice, ctx->stream));
+    }
+    CKL(cudaMemsetAsync(tcount, 0, 4 * N1, ctx->stream));
+    CKL(cudaMemsetAsync(tfill, 0, 4 * N1, ctx->stream));
+    CKL(launch_canonicalize(n, contiguous ? packed : nnz, dbeg, nullptr, dcol_in, m->rowptr, m->col,
+                            tcount, m->trowptr, m->tcol, tfill, scan_tmp, scan_bytes, dstatus,
+                            ctx->stream));
+    CKL(cudaMemcpyAsync(ctx->h_status, dstatus, 4, cudaMemcpyDeviceToHost, ctx->stream));
+    CKL(cudaStreamSynchronize(ctx->stream));
+#undef CKL
+    dev_free(ctx, sblk, stage);
+    rc = check_status(ctx);
+    if (rc) {
+        dev_free(ctx, blk, total);
+        delete m;
+        return rc;
+    }
+    *out = m;
+    return GSOFA_OK;
+}
+
+int gsofa_load_csr_files(gsofa_ctx* ctx, const char* beg_file, const char* end_file,
+                         const char* csr_file, gsofa_matrix** out) {
+    if (!ctx || !out || !beg_file || !end_file || !csr_file) return GSOFA_ERR_ARG;
+    std::string sc, sb, se;
+    if (read_file(csr_file, &sc)) return set_err(ctx, GSOFA_ERR_IO, "cannot read %s", csr_file);
+    size_t pos = 0;
+    bool bad = false;
+    int32_t hdr[2];
+    if (parse_ints(sc, &pos, 2, hdr, &bad) != 2 || bad || hdr[0] < 0 || hdr[1] < 0)
+        return set_err(ctx, GSOFA_ERR_IO, "%s: bad header (expected E N)", csr_file);
+    const int64_t E = hdr[0];
+    const int32_t n = hdr[1];
+    std::vector<int32_t> col((size_t)std::max<int64_t>(E, 1)), beg((size_t)n + 1), end((size_t)n + 1);
+    if (parse_ints(sc, &pos, E, col.data(), &bad) != E || bad)
+        return set_err(ctx, GSOFA_ERR_IO, "%s: expected %lld column ids", csr_file, (long long)E);
+    if (read_file(beg_file, &sb)) return set_err(ctx, GSOFA_ERR_IO, "cannot read %s", beg_file);
+    if (read_file(end_file, &se)) return set_err(ctx, GSOFA_ERR_IO, "cannot read %s", end_file);
+    pos = 0;
+    if (parse_ints(sb, &pos, n, beg.data(), &bad) != n || bad)
+        return set_err(ctx, GSOFA_ERR_IO, "%s: expected %d row starts", beg_file, n);
+    pos = 0;
+    if (parse_ints(se, &pos, n, end.data(), &bad) != n || bad)
+        return set_err(ctx, GSOFA_ERR_IO, "%s: expected %d row ends", end_file, n);
+    return gsofa_load_csr(ctx, n, E, beg.data(), end.data(), col.data(), out);
+}
+
+int gsofa_matrix_info(const gsofa_matrix* m, int32_t* n, int64_t* nnz) {
+    if (!m) return GSOFA_ERR_ARG;
+    if (n) *n = m->n;
+    if (nnz) *nnz = m->nnz;
+    return GSOFA_OK;
+}
+
+int gsofa_matrix_destroy(gsofa_matrix* m) {
+    if (!m) return GSOFA_ERR_ARG;
+    {
+        std::lock_guard<std::recursive_mutex> g(m->ctx->mu);
+        dev_free(m->ctx, m->rowptr, m->bytes);
+    }
+    delete m;
+    return GSOFA_OK;
+}
+
+int gsofa_factor_batch(gsofa_ctx* ctx, const gsofa_matrix* const* mats, int32_t count,
+                       const gsofa_opts* opts, gsofa_result** results) {
+    if (!ctx || count < 0 || (count > 0 && (!mats || !results))) return GSOFA_ERR_ARG;
+    std::lock_guard<std::recursive_mutex> g(ctx->mu);
+    gsofa_opts o;
+    if (opts) o = *opts; else gsofa_opts_default(&o);
+    int rc = validate_opts(ctx, &o);
+    if (rc) return rc;
+    for (int32_t i = 0; i < count; i++) {
+        results[i] = nullptr;
+        if (!mats[i] || mats[i]->ctx != ctx)
+            return set_err(ctx, GSOFA_ERR_ARG, "matrix %d is null or from another context", i);
+    }
+    if (cudaSetDevice(ctx->device) != cudaSuccess) return set_err(ctx, GSOFA_ERR_CUDA, "cudaSetDevice");
+    std::vector<gsofa_result*> res((size_t)count, nullptr);
+    for (int32_t i = 0; i < count; i++) {
+        rc = result_alloc(ctx, mats[i]->n, o.flags, o.max_supernode_size, &res[i]);
+        if (rc) {
+            for (auto* r : res) result_free(r);
+            return rc;
+        }
+    }
+    rc = run_factor(ctx, mats, count, &o, res.data());
+    if (rc) {
+        for (auto* r : res) result_free(r);
+        return rc;
+    }
+    for (int32_t i = 0; i < count; i++) results[i] = res[i];
+    return GSOFA_OK;
+}
+
+int gsofa_factor_symbolic(gsofa_ctx* ctx, const gsofa_matrix* mat, const gsofa_opts* opts,
+                          gsofa_result** out) {
+    if (!out) return GSOFA_ERR_ARG;
+    return gsofa_factor_batch(ctx, &mat, 1, opts, out);
+}
+
+int gsofa_result_counts(const gsofa_result* r, gsofa_counts* out) {
+    if (!r || !out) return GSOFA_ERR_ARG;
+    *out = r->counts;
+    return GSOFA_OK;
+}
+
+static int fetch(const gsofa_result* r, void* dst, const void* src, size_t bytes) {
+    if (!dst) return GSOFA_OK;
+    if (!src) return set_err(r->ctx, GSOFA_ERR_ARG, "requested array was not computed (option off)");
+    std::lock_guard<std::recursive_mutex> g(r->ctx->mu);
+    cudaError_t e = cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, r->ctx->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(r->ctx->stream);
+    if (e != cudaSuccess) return cuda_fail(r->ctx, e, "result fetch");
+    return GSOFA_OK;
+}
+
+int gsofa_result_row_counts(const gsofa_result* r, int32_t* nnz_u_row, int32_t* nz_row_u,
+                            int32_t* nnz_l_col, int32_t* nnz_l_row) {
+    if (!r) return GSOFA_ERR_ARG;
+    const size_t b = 4 * (size_t)r->n;
+    int rc;
+    if ((rc = fetch(r, nnz_u_row, r->nnz_u, b))) return rc;
+    if ((rc = fetch(r, nz_row_u, r->nz_row_u, b))) return rc;
+    if ((rc = fetch(r, nnz_l_col, r->nnz_lc, b))) return rc;
+    return fetch(r, nnz_l_row, r->nnz_lr, b);
+}
+
+int gsofa_result_digests(const gsofa_result* r, uint64_t* du, uint64_t* dlc, uint64_t* dlr) {
+    if (!r) return GSOFA_ERR_ARG;
+    const size_t b = 8 * (size_t)r->n;
+    int rc;
+    if ((rc = fetch(r, du, r->dig_u, b))) return rc;
+    if ((rc = fetch(r, dlc, r->dig_lc, b))) return rc;
+    return fetch(r, dlr, r->dig_lr, b);
+}
+
+int gsofa_result_lmask(const gsofa_result* r, uint32_t* mask4n) {
+    if (!r) return GSOFA_ERR_ARG;
+    return fetch(r, mask4n, r->lmask, 16 * (size_t)r->n);
+}
+
+int gsofa_result_supernodes(const gsofa_result* r, int8_t* flags, int32_t* boundaries, int64_t cap,
+                            int64_t* count) {
+    if (!r) return GSOFA_ERR_ARG;
+    if (!(r->flags & GSOFA_SUPERNODES))
+        return set_err(r->ctx, GSOFA_ERR_ARG, "supernode detection was not requested");
+    std::vector<int8_t> f((size_t)r->n);
+    int rc = fetch(r, f.data(), r->sflags, (size_t)r->n);
+    if (rc) return rc;
+    if (flags) memcpy(flags, f.data(), (size_t)r->n);
+    int64_t k = 0;
+    for (int32_t v = 0; v < r->n; v++) {
+        if (f[v]) {
+            if (boundaries && k < cap) boundaries[k] = v;
+            k++;
+        }
+    }
+    if (count) *count = k;
+    return GSOFA_OK;
+}
+
+static int fetch_pattern(const gsofa_result* r, const int64_t* dptr, const int32_t* dids,
+                         int64_t* ptr, int32_t* ids, int64_t cap) {
+    if (!(r->flags & GSOFA_PATTERN) || !dptr)
+        return set_err(r->ctx, GSOFA_ERR_ARG, "pattern was not requested (GSOFA_PATTERN)");
+    std::vector<int64_t> p((size_t)r->n + 1);
+    int rc = fetch(r, p.data(), dptr, 8 * ((size_t)r->n + 1));
+    if (rc) return rc;
+    if (ptr) memcpy(ptr, p.data(), 8 * ((size_t)r->n + 1));
+    if (ids) {
+        if (cap < p[(size_t)r->n])
+            return set_err(r->ctx, GSOFA_ERR_ARG, "id buffer holds %lld, needs %lld", (long long)cap,
+                           (long long)p[(size_t)r->n]);
+        if (p[(size_t)r->n] > 0) rc = fetch(r, ids, dids, 4 * (size_t)p[(size_t)r->n]);
+    }
+    return rc;
+}
+
+int gsofa_result_pattern_u(const gsofa_result* r, int64_t* ptr, int32_t* cols, int64_t cap) {
+    if (!r) return GSOFA_ERR_ARG;
+    return fetch_pattern(r, r->uptr, r->ucols, ptr, cols, cap);
+}
+
+int gsofa_result_pattern_l(const gsofa_result* r, int64_t* ptr, int32_t* rows, int64_t cap) {
+    if (!r) return GSOFA_ERR_ARG;
+    return fetch_pattern(r, r->lptr, r->lrows, ptr, rows, cap);
+}
+
+int gsofa_result_destroy(gsofa_result* r) {
+    if (!r) return GSOFA_ERR_ARG;
+    result_free(r);
+    return GSOFA_OK;
+}
+
+// The reference's two command lines (SOA argc == 11, :2532-2545; SPO argc == 6,
+// symbfact.cuh:1557-1571), folded onto one device.
+int gsofa_symbfact_min_id(int argc, char** argv, int rank, uint64_t* fill_count, double* time_ms,
+                          int32_t* n_supernodes, uint64_t* teps_edges) {
+    if (!argv || (argc != 11 && argc != 6)) return GSOFA_ERR_ARG;
+    gsofa_opts o;
+    gsofa_opts_default(&o);
+    size_t budget = 0;
+    if (argc == 11) {
+        int mss = atoi(argv[5]);
+        if (mss <= 0) return GSOFA_ERR_ARG;
+        o.max_supernode_size = mss;
+    } else {
+        double gb = atof(argv[5]);
+        if (gb < 0) return GSOFA_ERR_ARG;
+        // the reference's pool holds its 6 work arrays; here the budget bounds
+        // everything the context allocates (matrix, workspace, results)
+        budget = gb > 0 ? (size_t)(gb * 1024.0 * 1024.0 * 1024.0) : 0;
+        o.flags &= ~(uint32_t)GSOFA_SUPERNODES;
+    }
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= 0) return GSOFA_ERR_CUDA;
+    gsofa_ctx* ctx = nullptr;
+    int rc = gsofa_create(rank % ndev, budget, &ctx);
+    if (rc) return rc;
+    gsofa_matrix* m = nullptr;
+    rc = gsofa_load_csr_files(ctx, argv[1], argv[2], argv[3], &m);
+    if (rc) {
+        fprintf(stderr, "gsofa: %s\n", gsofa_last_error(ctx));
+        gsofa_destroy(ctx);
+        return rc;
+    }
+    gsofa_result* r = nullptr;
+    rc = gsofa_factor_symbolic(ctx, m, &o, &r);
+    if (rc) {
+        fprintf(stderr, "gsofa: %s\n", gsofa_last_error(ctx));
+        gsofa_matrix_destroy(m);
+        gsofa_destroy(ctx);
+        return rc;
+    }
+    gsofa_counts c;
+    gsofa_result_counts(r, &c);
+    if (fill_count) *fill_count = c.fill_count;
+    if (time_ms) *time_ms = c.ms_device;
+    if (n_supernodes) *n_supernodes = (int32_t)c.n_supernodes;
+    if (teps_edges) *teps_edges = c.edges_alg;
+    gsofa_result_destroy(r);
+    gsofa_matrix_destroy(m);
+    gsofa_destroy(ctx);
+    return GSOFA_OK;
+}
+
+}  // extern "C"

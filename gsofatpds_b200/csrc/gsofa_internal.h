@@ -1,0 +1,85 @@
+// Internal structures shared by the host library and the CUDA kernels.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace gsofa {
+
+// Device-side error word bits (read back by the host after every launch).
+enum : int32_t {
+    DEV_ERR_COL_RANGE = 1,   // a column id outside [0, n)
+    DEV_ERR_ROW_RANGE = 2,   // a row interval outside [0, nnz) or begin > end
+    DEV_ERR_QUEUE = 4,       // a traversal queue write past its bound
+};
+
+// Counter slots of MatOut::counters.
+enum : int {
+    CNT_FILLS = 0,
+    CNT_EDGES_ALG = 1,
+    CNT_VERTS_ALG = 2,
+    CNT_EDGES_TRAV = 3,
+    CNT_NSUP = 4,
+    CNT_NNZ_U = 5,
+    CNT_NNZ_L = 6,
+    CNT_SLOTS = 8,
+};
+
+// One matrix as the traversal sees it: A by rows and A^T by rows, both with
+// contiguous rows, plus the per-row outputs.
+struct MatDesc {
+    int32_t n;
+    int32_t flags;              // GSOFA_* bits
+    const int32_t* rowptr;      // n+1
+    const int32_t* col;
+    const int32_t* trowptr;     // n+1 (A^T)
+    const int32_t* tcol;
+    int32_t* nnz_u;             // n: |U row|
+    int32_t* nz_row_u;          // n: reference nz_row_U counter
+    uint64_t* dig_u;            // n (or null)
+    int32_t* nnz_lc;            // n: |L column|
+    uint64_t* dig_lc;           // n (or null)
+    uint32_t* lmask;            // 4n: L(f+1+j, f) bits
+    int32_t* nnz_lr;            // n or null (L row scatter)
+    uint64_t* dig_lr;           // n or null
+    unsigned long long* counters;  // CNT_SLOTS
+    const int64_t* uptr;        // pattern pass: U row pointers (n+1) or null
+    int32_t* ucols;
+    const int64_t* lptr;        // pattern pass: L column pointers (n+1) or null
+    int32_t* lrows;
+    long long item_base;        // first work item of this matrix
+};
+
+struct TraverseLaunch {
+    const MatDesc* mats;        // device array
+    int32_t nmats;
+    long long total_items;
+    unsigned long long* work_counter;  // device, zeroed before launch
+    int32_t* queue;             // grid * queue_stride ints
+    long long queue_stride;
+    uint32_t* gbitmap;          // grid * bitmap_words (global-bitmap variant) or null
+    long long bitmap_words;     // words per bitmap (covers max n + padding)
+    int32_t* status;            // device error word
+    int pattern_pass;           // 1: write patterns instead of counting
+};
+
+// Launch helpers (gsofa_kernels.cu).  All asynchronous on `stream`.
+int traverse_block_sizes(int* sizes, int max_sizes);
+// Returns the resident CTAs per SM for the given configuration (0 = cannot run).
+int traverse_occupancy(int block, bool smem_bitmap, size_t smem_bytes);
+cudaError_t launch_traverse(const TraverseLaunch& L, int block, int grid, bool smem_bitmap,
+                            size_t smem_bytes, cudaStream_t stream);
+cudaError_t launch_canonicalize(int32_t n, long long nnz, const int32_t* beg, const int32_t* end,
+                                const int32_t* col_in, int32_t* rowptr, int32_t* col_out,
+                                int32_t* tcount, int32_t* trowptr, int32_t* tcol, int32_t* tfill,
+                                void* scan_tmp, size_t scan_tmp_bytes, int32_t* status,
+                                cudaStream_t stream);
+size_t canonicalize_scan_bytes(int32_t n);
+cudaError_t launch_supernodes(int32_t n, int32_t mss, const int32_t* nz_row_u,
+                              const uint32_t* lmask, int8_t* flags,
+                              unsigned long long* counters, cudaStream_t stream);
+cudaError_t launch_pattern_ptrs(int32_t n, const int32_t* nnz_u, const int32_t* nnz_lc,
+                                int64_t* uptr, int64_t* lptr, void* scan_tmp,
+                                size_t scan_tmp_bytes, cudaStream_t stream);
+size_t pattern_scan_bytes(int32_t n);
+
+}  // namespace gsofa

@@ -1,0 +1,162 @@
+/*
+ * gsofa.h -- C-ABI of the B200 symbolic-LU ("fill-path") engine.
+ *
+ * The reference (gSoFaTPDS) is an executable, not a library: its entry is
+ *   void symbfact_min_id(int argc, char** argv, int rank, ull_t& fill_count,
+ *                        double& time, int& N_supernodes, ull_t& TEPS)
+ *   (gSoFa_SOAComparison/symbfact_warp_centric_new_scheduling.cuh:2529;
+ *    SpaceOptimization/symbfact.cuh:1553 has the same call without the last two)
+ * called from main() (gSoFa_SOAComparison/main.cu:20-64).  This header splits
+ * that monolith into handles so a caller (CLI, test harness, benchmark,
+ * serving loop, or another language through its FFI) can load a matrix once,
+ * keep it device-resident and factor it repeatedly.  Every function returns a
+ * status code; none of them exits or aborts the process (the reference's
+ * H_ERR macro calls exit(EXIT_FAILURE), barrier.cuh:11-20).
+ *
+ * Plain C types only: no CUDA or torch types appear in the signatures.
+ */
+#ifndef GSOFA_H
+#define GSOFA_H
+#include <stddef.h>
+#include <stdint.h>
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes --------------------------------------------------------- */
+#define GSOFA_OK 0
+#define GSOFA_ERR_ARG 1          /* invalid argument or malformed CSR        */
+#define GSOFA_ERR_IO 2           /* file missing or unparsable               */
+#define GSOFA_ERR_OOM_BUDGET 3   /* would exceed the context's memory budget */
+#define GSOFA_ERR_TIMEOUT 4      /* a bounded device wait gave up            */
+#define GSOFA_ERR_OVERFLOW 5     /* a device queue bound was exceeded        */
+#define GSOFA_ERR_CUDA 6         /* CUDA runtime error (message in last_error) */
+#define GSOFA_ERR_UNSUPPORTED 7  /* size or option outside what is built     */
+#define GSOFA_ERR_BUSY 8         /* serving queue full / ticket not finished */
+
+typedef struct gsofa_ctx gsofa_ctx;
+typedef struct gsofa_matrix gsofa_matrix;
+typedef struct gsofa_result gsofa_result;
+
+/* ---- options -------------------------------------------------------------- */
+#define GSOFA_SUPERNODES (1u << 0)  /* detect supernodes (reference SOA :1790-2123) */
+#define GSOFA_L_ROW_STATS (1u << 1) /* also per-row L counts + digests (scatter)     */
+#define GSOFA_PATTERN (1u << 2)     /* materialise L (by columns) and U (by rows)    */
+#define GSOFA_DIGESTS (1u << 3)     /* per-row/column 64-bit column-set digests      */
+/* Diagnostic: keep the traversal's seen-bitmap in global memory even when
+ * it fits in shared memory (the variant used for orders above ~1.8M). */
+#define GSOFA_FORCE_GLOBAL_BITMAP (1u << 30)
+
+typedef struct gsofa_opts {
+    /* rows per supernode chunk; the reference's max_supernode_size, argv[5]
+     * of the SOA command line (symbfact_warp_centric_new_scheduling.cuh:2540) */
+    int32_t max_supernode_size;
+    /* threads cooperating on one source traversal (CTA size: 128..1024,
+     * multiple of 32); 0 = autotuned */
+    int32_t threads_per_source;
+    /* concurrent source traversals (CTAs); 0 = as many as fit on the GPU.
+     * The reference's N_src_group (Compute_Src_group, :1031-1048) */
+    int32_t sources_in_flight;
+    uint32_t flags; /* GSOFA_* option bits */
+} gsofa_opts;
+
+/* Defaults: max_supernode_size 128, autotuned CTA size, GPU-filling
+ * concurrency, flags = GSOFA_SUPERNODES | GSOFA_DIGESTS. */
+int gsofa_opts_default(gsofa_opts* opts);
+
+/* ---- context -------------------------------------------------------------- */
+/* One context per device.  budget_bytes bounds every device allocation the
+ * context makes (matrices, workspace, results); 0 = 90% of free memory.
+ * Replaces the reference's cudaSetDevice + per-GPU allocation
+ * (Allocate_Initialize, :2296-2472; SPO pool, symbfact.cuh:1683-1687). */
+int gsofa_create(int device, size_t budget_bytes, gsofa_ctx** out);
+int gsofa_destroy(gsofa_ctx* ctx);
+/* Message for the last failing call on this context (never NULL). */
+const char* gsofa_last_error(const gsofa_ctx* ctx);
+const char* gsofa_status_string(int status);
+/* Launch on this CUDA stream (a cudaStream_t passed as void*); NULL = the
+ * context's own stream. */
+int gsofa_set_stream(gsofa_ctx* ctx, void* cuda_stream);
+/* Device bytes currently held by the context. */
+int gsofa_memory_used(const gsofa_ctx* ctx, size_t* bytes);
+
+/* ---- matrices (replaces the ASCII ingest, :2567-2616 / symbfact.cuh:1591-1640) */
+/* Row v of A is col[row_begin[v] .. row_end[v]).  Rows may be stored in any
+ * order and need not be contiguous or sorted (the reference's BC input is
+ * neither).  Host pointers; the matrix is copied to the device. */
+int gsofa_load_csr(gsofa_ctx* ctx, int32_t n, int64_t nnz, const int32_t* row_begin,
+                   const int32_t* row_end, const int32_t* col, gsofa_matrix** out);
+/* The reference's three ASCII files: csr = "E N" then E column ids,
+ * beg / end = n ids each. */
+int gsofa_load_csr_files(gsofa_ctx* ctx, const char* beg_file, const char* end_file,
+                         const char* csr_file, gsofa_matrix** out);
+int gsofa_matrix_info(const gsofa_matrix* mat, int32_t* n, int64_t* nnz);
+int gsofa_matrix_destroy(gsofa_matrix* mat);
+
+/* ---- factorization (replaces the group loop :2965-3218 and its kernels) --- */
+/* Synchronous: returns when the result is complete on the device. */
+int gsofa_factor_symbolic(gsofa_ctx* ctx, const gsofa_matrix* mat, const gsofa_opts* opts,
+                          gsofa_result** out);
+/* Many matrices of uneven size in one persistent launch; results[i] is the
+ * result of mats[i] (identical to factoring it alone). */
+int gsofa_factor_batch(gsofa_ctx* ctx, const gsofa_matrix* const* mats, int32_t count,
+                       const gsofa_opts* opts, gsofa_result** results);
+
+typedef struct gsofa_counts {
+    int32_t n;
+    int32_t reserved;
+    uint64_t fill_count;      /* reference "Number of fill-ins detected"        */
+    uint64_t nnz_l;           /* strictly-lower entries of L+U (A's + fills)     */
+    uint64_t nnz_u;           /* strictly-upper entries of L+U                   */
+    uint64_t nnz_lu;          /* nnz_l + nnz_u + n (full diagonal)               */
+    int64_t n_supernodes;     /* reference's printed count (detected + 1), -1 if off */
+    uint64_t edges_alg;       /* sum over sources s of the degrees of the vertices
+                               * < s reachable from s through vertices < s      */
+    uint64_t vertices_alg;    /* number of such (source, vertex) pairs          */
+    uint64_t edges_traversed; /* edge inspections this engine made (A and A^T)  */
+    double ms_device;         /* device time of the factorization (CUDA events) */
+    double ms_traverse;       /* device time of the traversal kernel alone      */
+} gsofa_counts;
+int gsofa_result_counts(const gsofa_result* res, gsofa_counts* out);
+
+/* Per-row / per-column counts (host buffers of n entries; any may be NULL):
+ *   nnz_u_row[v]  distinct strictly-upper entries of row v of U
+ *   nz_row_u[v]   the reference's nz_row_U counter (SOA :895-903, :985-992)
+ *   nnz_l_col[v]  distinct strictly-lower entries of column v of L
+ *   nnz_l_row[v]  distinct strictly-lower entries of row v (needs GSOFA_L_ROW_STATS) */
+int gsofa_result_row_counts(const gsofa_result* res, int32_t* nnz_u_row, int32_t* nz_row_u,
+                            int32_t* nnz_l_col, int32_t* nnz_l_row);
+/* Column-set digests: sum mod 2^64 of splitmix64(column id) over the set. */
+int gsofa_result_digests(const gsofa_result* res, uint64_t* dig_u_row, uint64_t* dig_l_col,
+                         uint64_t* dig_l_row);
+/* Supernode partition: flags[v] (n bytes) = 1 row starts a supernode, 2 a
+ * supernode is counted at this row without moving the first row (the
+ * reference's split rule, SOA :2043-2052), 0 row extends the current one.
+ * boundaries: rows with a non-zero flag, ascending, up to cap entries;
+ * *count gets the total.  Any pointer may be NULL. */
+int gsofa_result_supernodes(const gsofa_result* res, int8_t* flags, int32_t* boundaries,
+                            int64_t cap, int64_t* count);
+/* 128-bit masks per column f: bit j of word j/32 set iff L(f+1+j, f) != 0. */
+int gsofa_result_lmask(const gsofa_result* res, uint32_t* mask4n);
+/* Materialised pattern (needs GSOFA_PATTERN).  U by rows: ptr[n+1] and the
+ * sorted column ids of each row; L by columns: ptr[n+1] and the sorted row
+ * ids of each column.  cap = capacity of the id buffer; pass ids = NULL to
+ * get ptr only. */
+int gsofa_result_pattern_u(const gsofa_result* res, int64_t* ptr, int32_t* cols, int64_t cap);
+int gsofa_result_pattern_l(const gsofa_result* res, int64_t* ptr, int32_t* rows, int64_t cap);
+int gsofa_result_destroy(gsofa_result* res);
+
+/* ---- reference-shaped entry point ------------------------------------------ */
+/* Same argument layouts as the reference executables:
+ *   SOA: exe beg end csr num_process max_supernode_size percent_cat0
+ *        percent_cat2 N_blocks_source_cat2 N_GPU_Node N_src_group  (argc == 11)
+ *   SPO: exe beg end csr N_virtualGPU total_memory_GB              (argc == 6)
+ * Outputs mirror symbfact_min_id's reference parameters; teps_edges gets
+ * edges_alg.  Process/GPU counts are accepted and folded onto one device. */
+int gsofa_symbfact_min_id(int argc, char** argv, int rank, uint64_t* fill_count,
+                          double* time_ms, int32_t* n_supernodes, uint64_t* teps_edges);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* GSOFA_H */
