@@ -33,6 +33,7 @@ WORKLOADS = {
     "circuit_like": "circuit-like n=659033 ~5.84M nnz, Zipf(1.2) long links, symmetric permutation, mss 128",
     "random_extra": "n=20000 diagonal+tridiagonal+3 uniform columns/row, mss 128",
     "grid3d_64": "64^3 7-point grid, nested-dissection order, mss 256",
+    "circuit_like_100k": "circuit-like n=100000 ~0.89M nnz (profiling size), mss 128",
 }
 
 
@@ -44,6 +45,8 @@ def make_workload(name):
         return gen.random_extra(20000, 3, seed=1), 128
     if name == "grid3d_64":
         return gen.grid_nd((64, 64, 64), "7"), 256
+    if name == "circuit_like_100k":
+        return gen.circuit_like(n=100000, target_nnz=int(5830000 * 100000 / 659033)), 128
     raise SystemExit("unknown workload " + name)
 
 

@@ -25,6 +25,7 @@ L_ROW_STATS = 1 << 1
 PATTERN = 1 << 2
 DIGESTS = 1 << 3
 FORCE_GLOBAL_BITMAP = 1 << 30
+NO_MERGE = 1 << 29
 
 # Every function the header declares (checked by the CPU test-suite).
 EXPORTS = [
@@ -42,7 +43,14 @@ class Opts(ctypes.Structure):
     _fields_ = [("max_supernode_size", ctypes.c_int32),
                 ("threads_per_source", ctypes.c_int32),
                 ("sources_in_flight", ctypes.c_int32),
-                ("flags", ctypes.c_uint32)]
+                ("flags", ctypes.c_uint32),
+                ("bu_alpha", ctypes.c_int32),
+                ("bu_beta", ctypes.c_int32),
+                ("heavy_row", ctypes.c_int32),
+                ("bu_min_source", ctypes.c_int32),
+                ("chunk_sources", ctypes.c_int32),
+                ("cached_closures", ctypes.c_int32),
+                ("reserved", ctypes.c_int32 * 2)]
 
 
 class Counts(ctypes.Structure):

@@ -84,13 +84,22 @@ class Context:
 
     @staticmethod
     def opts(max_supernode_size=128, threads_per_source=0, sources_in_flight=0,
-             supernodes=True, digests=True, l_row_stats=False, pattern=False):
+             supernodes=True, digests=True, l_row_stats=False, pattern=False,
+             bu_alpha=0, bu_beta=0, heavy_row=0, bu_min_source=0, chunk_sources=0,
+             merge=True, cached_closures=0):
         o = C.Opts()
+        o.cached_closures = int(cached_closures)
+        o.chunk_sources = int(chunk_sources)
+        o.bu_min_source = int(bu_min_source)
+        o.bu_alpha = int(bu_alpha)
+        o.bu_beta = int(bu_beta)
+        o.heavy_row = int(heavy_row)
         o.max_supernode_size = int(max_supernode_size)
         o.threads_per_source = int(threads_per_source)
         o.sources_in_flight = int(sources_in_flight)
         o.flags = ((C.SUPERNODES if supernodes else 0) | (C.DIGESTS if digests else 0) |
-                   (C.L_ROW_STATS if l_row_stats else 0) | (C.PATTERN if pattern else 0))
+                   (C.L_ROW_STATS if l_row_stats else 0) | (C.PATTERN if pattern else 0) |
+                   (0 if merge else C.NO_MERGE))
         return o
 
     def factor(self, mat, **kw):

@@ -26,6 +26,7 @@ struct gsofa_ctx {
     int device = 0;
     int sm_count = 0;
     int smem_optin = 0;
+    int smem_per_sm = 0;
     size_t budget = 0;
     size_t used = 0;
     cudaStream_t own_stream = nullptr;
@@ -42,6 +43,8 @@ struct gsofa_ctx {
     size_t queue_bytes = 0;
     void* gbitmap = nullptr;
     size_t gbitmap_bytes = 0;
+    void* gprev = nullptr;
+    size_t gprev_bytes = 0;
     void* small = nullptr;  // work counter (8 B) + status (4 B)
     void* scan_tmp = nullptr;
     size_t scan_tmp_bytes = 0;
@@ -55,6 +58,7 @@ struct gsofa_matrix {
     int32_t* col = nullptr;
     int32_t* trowptr = nullptr;
     int32_t* tcol = nullptr;
+    int32_t* wdeg = nullptr;
     size_t bytes = 0;
 };
 
@@ -150,11 +154,26 @@ size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
 
 long long bitmap_words(int32_t n) { return (((long long)n + 31) >> 5) + 6; }
 
-int default_block(int32_t nmax) {
-    // Measured-on-B200 defaults are refined by the Python autotuner; these
-    // are the starting points: small orders have short searches.
-    if (nmax < 8192) return 256;
-    return 512;
+// Direction-switch and row-split defaults of the traversal (see
+// gsofa_kernels.cu); the autotuner overrides them per call.
+constexpr int kDefaultBuAlpha = 0;  // top-down only unless a caller asks
+constexpr int kDefaultBuBeta = 24;
+constexpr int kBuMinSource = 2048;
+constexpr int kDefaultHeavyRow = 64;
+constexpr int kDefaultChunk = 64;
+constexpr int kDefaultRing = 16;
+
+// Default CTA size: about 1024 resident threads per SM (the kernel is held
+// to 64 registers), given how many shared-memory bitmaps fit per SM.
+// Measured on B200: 256-thread CTAs are fastest whenever 4 fit, else fewer,
+// larger CTAs.
+int default_block(int32_t nmax, int smem_per_sm) {
+    const long long words = (((long long)nmax + 31) >> 5) + 6;
+    const long long per_cta = ((words * 4 + 15) & ~15ll) + 8 * 1024;
+    long long fit = smem_per_sm / per_cta;
+    if (fit >= 4) return 256;
+    if (fit >= 2) return 512;
+    return 1024;
 }
 
 struct LaunchCfg {
@@ -166,7 +185,8 @@ struct LaunchCfg {
 };
 
 int plan_launch(gsofa_ctx* ctx, int32_t nmax, const gsofa_opts* o, LaunchCfg* c) {
-    c->block = o->threads_per_source > 0 ? o->threads_per_source : default_block(nmax);
+    c->block = o->threads_per_source > 0 ? o->threads_per_source
+                                         : default_block(nmax, ctx->smem_per_sm);
     if (c->block != 128 && c->block != 256 && c->block != 512 && c->block != 1024)
         return set_err(ctx, GSOFA_ERR_ARG, "threads_per_source must be 128, 256, 512 or 1024");
     c->words = bitmap_words(nmax);
@@ -277,6 +297,7 @@ MatDesc make_desc(const gsofa_matrix* m, const gsofa_result* r, long long base) 
     d.col = m->col;
     d.trowptr = m->trowptr;
     d.tcol = m->tcol;
+    d.wdeg = m->wdeg;
     d.nnz_u = r->nnz_u;
     d.nz_row_u = r->nz_row_u;
     d.dig_u = r->dig_u;
@@ -300,9 +321,10 @@ int run_factor(gsofa_ctx* ctx, const gsofa_matrix* const* mats, int32_t count,
                const gsofa_opts* o, gsofa_result** res) {
     int32_t nmax = 0;
     long long items = 0;
+    const long long chunk = o->chunk_sources > 0 ? o->chunk_sources : kDefaultChunk;
     for (int32_t i = 0; i < count; i++) {
         nmax = std::max(nmax, mats[i]->n);
-        items += 2ll * mats[i]->n;
+        items += 2ll * ((mats[i]->n + chunk - 1) / chunk);
     }
     LaunchCfg cfg;
     int rc = plan_launch(ctx, std::max(nmax, 1), o, &cfg);
@@ -313,12 +335,21 @@ int run_factor(gsofa_ctx* ctx, const gsofa_matrix* const* mats, int32_t count,
         rc = ensure(ctx, &ctx->gbitmap, &ctx->gbitmap_bytes, (size_t)cfg.grid * (size_t)cfg.words * 4);
         if (rc) return rc;
     }
+    const bool merge = !(o->flags & GSOFA_NO_MERGE);
+    int ring = o->cached_closures > 0 ? o->cached_closures : kDefaultRing;
+    if (ring > 32) ring = 32;
+    while (ring & (ring - 1)) ring &= ring - 1;  // power of 2
+    if (merge) {
+        rc = ensure(ctx, &ctx->gprev, &ctx->gprev_bytes,
+                    (size_t)cfg.grid * (size_t)ring * (size_t)cfg.words * 4);
+        if (rc) return rc;
+    }
     // matrix descriptors
     std::vector<MatDesc> descs((size_t)count);
     long long base = 0;
     for (int32_t i = 0; i < count; i++) {
         descs[i] = make_desc(mats[i], res[i], base);
-        base += 2ll * mats[i]->n;
+        base += 2ll * ((mats[i]->n + chunk - 1) / chunk);
     }
     void* ddesc = nullptr;
     rc = dev_alloc(ctx, sizeof(MatDesc) * (size_t)count, &ddesc);
@@ -340,6 +371,14 @@ int run_factor(gsofa_ctx* ctx, const gsofa_matrix* const* mats, int32_t count,
     L.bitmap_words = cfg.words;
     L.status = dstatus;
     L.pattern_pass = 0;
+    L.bu_alpha = o->bu_alpha > 0 ? o->bu_alpha : (o->bu_alpha < 0 ? 0 : kDefaultBuAlpha);
+    L.bu_beta = o->bu_beta > 0 ? o->bu_beta : kDefaultBuBeta;
+    L.bu_min_src = o->bu_min_source > 0 ? o->bu_min_source : kBuMinSource;
+    L.gprev = reinterpret_cast<uint32_t*>(ctx->gprev);
+    L.merge = merge ? 1 : 0;
+    L.ring = ring;
+    L.chunk = o->chunk_sources > 0 ? o->chunk_sources : kDefaultChunk;
+    L.heavy_len = o->heavy_row > 0 ? ((o->heavy_row + 3) & ~3) : kDefaultHeavyRow;
 
     CK(cudaEventRecord(ctx->ev0, ctx->stream));
     if (items > 0) CK(launch_traverse(L, cfg.block, cfg.grid, cfg.smem_bitmap, cfg.smem, ctx->stream));
@@ -428,7 +467,8 @@ int run_factor(gsofa_ctx* ctx, const gsofa_matrix* const* mats, int32_t count,
 int validate_opts(gsofa_ctx* ctx, const gsofa_opts* o) {
     if (o->max_supernode_size <= 0)
         return set_err(ctx, GSOFA_ERR_ARG, "max_supernode_size must be positive");
-    if (o->threads_per_source < 0 || o->sources_in_flight < 0)
+    if (o->threads_per_source < 0 || o->sources_in_flight < 0 || o->chunk_sources < 0 ||
+        o->cached_closures < 0)
         return set_err(ctx, GSOFA_ERR_ARG, "negative launch option");
     return GSOFA_OK;
 }
@@ -492,6 +532,13 @@ int gsofa_opts_default(gsofa_opts* o) {
     o->threads_per_source = 0;
     o->sources_in_flight = 0;
     o->flags = GSOFA_SUPERNODES | GSOFA_DIGESTS;
+    o->bu_alpha = 0;
+    o->bu_beta = 0;
+    o->heavy_row = 0;
+    o->bu_min_source = 0;
+    o->chunk_sources = 0;
+    o->cached_closures = 0;
+    o->reserved[0] = o->reserved[1] = 0;
     return GSOFA_OK;
 }
 
@@ -523,6 +570,7 @@ int gsofa_create(int device, size_t budget_bytes, gsofa_ctx** out) {
     if (e != cudaSuccess) return fail(e);
     cudaDeviceGetAttribute(&ctx->sm_count, cudaDevAttrMultiProcessorCount, device);
     cudaDeviceGetAttribute(&ctx->smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device);
+    cudaDeviceGetAttribute(&ctx->smem_per_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, device);
     size_t fr = 0, tot = 0;
     if ((e = cudaMemGetInfo(&fr, &tot)) != cudaSuccess) return fail(e);
     ctx->budget = budget_bytes ? budget_bytes : (size_t)(0.9 * (double)fr);
@@ -553,6 +601,7 @@ int gsofa_destroy(gsofa_ctx* ctx) {
         cudaSetDevice(ctx->device);
         dev_free(ctx, ctx->queue, ctx->queue_bytes);
         dev_free(ctx, ctx->gbitmap, ctx->gbitmap_bytes);
+        dev_free(ctx, ctx->gprev, ctx->gprev_bytes);
         dev_free(ctx, ctx->scan_tmp, ctx->scan_tmp_bytes);
         dev_free(ctx, ctx->small, 256);
         cudaStreamSynchronize(ctx->stream);
@@ -599,31 +648,35 @@ int gsofa_load_csr(gsofa_ctx* ctx, int32_t n, int64_t nnz, const int32_t* row_be
     if (nnz > 0 && !col) return set_err(ctx, GSOFA_ERR_ARG, "null column array");
     if (nnz > INT32_MAX) return set_err(ctx, GSOFA_ERR_UNSUPPORTED, "nnz above 2^31-1");
     if (cudaSetDevice(ctx->device) != cudaSuccess) return set_err(ctx, GSOFA_ERR_CUDA, "cudaSetDevice");
-    // host: row pointers of the packed layout, and a contiguity test
-    std::vector<int32_t> rowptr((size_t)n + 1);
-    int64_t acc = 0;
-    bool contiguous = true;
+    // host: padded row pointers of A.  Row v gets a multiple of 4 slots; the
+    // number of padding slots of row v sits in the low 2 bits of rp[v+1].
+    std::vector<int32_t> rp((size_t)n + 1);
+    int64_t acc = 0, real = 0;
+    rp[0] = 0;
     for (int32_t v = 0; v < n; v++) {
         const int64_t b = row_begin[v], e = row_end[v];
         if (b < 0 || e < b || e > nnz)
             return set_err(ctx, GSOFA_ERR_ARG, "row %d interval [%lld,%lld) outside [0,%lld)", v,
                            (long long)b, (long long)e, (long long)nnz);
-        if (b != acc) contiguous = false;
-        rowptr[v] = (int32_t)acc;
-        acc += e - b;
-        if (acc > INT32_MAX) return set_err(ctx, GSOFA_ERR_UNSUPPORTED, "packed nnz above 2^31-1");
+        const int64_t d = e - b, pd = (d + 3) & ~(int64_t)3;
+        real += d;
+        acc += pd;
+        if (acc > INT32_MAX - 4 || real + 3ll * n > INT32_MAX - 4)
+            return set_err(ctx, GSOFA_ERR_UNSUPPORTED, "padded nnz above 2^31");
+        rp[(size_t)v + 1] = (int32_t)(acc | (pd - d));
     }
-    rowptr[(size_t)n] = (int32_t)acc;
-    const int64_t packed = acc;
+    const int64_t padded = acc;
 
     gsofa_matrix* m = new (std::nothrow) gsofa_matrix();
     if (!m) return set_err(ctx, GSOFA_ERR_OOM_BUDGET, "host allocation failed");
     m->ctx = ctx;
     m->n = n;
-    m->nnz = packed;
+    m->nnz = real;
     const size_t N1 = (size_t)n + 1;
-    const size_t P = (size_t)std::max<int64_t>(packed, 1);
-    size_t total = align256(4 * N1) * 2 + align256(4 * P) * 2;
+    const size_t PA = (size_t)std::max<int64_t>(padded, 4);
+    const size_t PT = (size_t)std::max<int64_t>(real + 3ll * n, 4);  // bound for A^T
+    const size_t NW = (size_t)(((int64_t)n + 31) >> 5) + 1;
+    size_t total = align256(4 * N1) * 2 + align256(4 * PA) + align256(4 * PT) + align256(4 * NW);
     void* blk = nullptr;
     int rc = dev_alloc(ctx, total, &blk);
     if (rc) { delete m; return rc; }
@@ -632,12 +685,14 @@ int gsofa_load_csr(gsofa_ctx* ctx, int32_t n, int64_t nnz, const int32_t* row_be
     m->rowptr = reinterpret_cast<int32_t*>(b);
     m->trowptr = reinterpret_cast<int32_t*>(b + align256(4 * N1));
     m->col = reinterpret_cast<int32_t*>(b + 2 * align256(4 * N1));
-    m->tcol = reinterpret_cast<int32_t*>(b + 2 * align256(4 * N1) + align256(4 * P));
+    m->tcol = reinterpret_cast<int32_t*>(b + 2 * align256(4 * N1) + align256(4 * PA));
+    m->wdeg = reinterpret_cast<int32_t*>(b + 2 * align256(4 * N1) + align256(4 * PA) +
+                                         align256(4 * PT));
 
-    // staging: raw input (beg, col_in) + transpose counters
+    // staging: raw input (beg, col_in) and the transpose's counters
     const size_t Nin = (size_t)std::max<int64_t>(nnz, 1);
     size_t scan_bytes = canonicalize_scan_bytes(n);
-    size_t stage = align256(4 * N1) + (contiguous ? 0 : align256(4 * Nin)) + align256(4 * N1) * 2 +
+    size_t stage = align256(4 * N1) + align256(4 * Nin) + align256(4 * N1) * 3 +
                    align256(scan_bytes) + 256;
     void* sblk = nullptr;
     rc = dev_alloc(ctx, stage, &sblk);
@@ -645,14 +700,13 @@ int gsofa_load_csr(gsofa_ctx* ctx, int32_t n, int64_t nnz, const int32_t* row_be
     char* s = reinterpret_cast<char*>(sblk);
     int32_t* dbeg = reinterpret_cast<int32_t*>(s);
     s += align256(4 * N1);
-    int32_t* dcol_in = m->col;
-    if (!contiguous) {
-        dcol_in = reinterpret_cast<int32_t*>(s);
-        s += align256(4 * Nin);
-    }
+    int32_t* dcol_in = reinterpret_cast<int32_t*>(s);
+    s += align256(4 * Nin);
     int32_t* tcount = reinterpret_cast<int32_t*>(s);
     s += align256(4 * N1);
     int32_t* tfill = reinterpret_cast<int32_t*>(s);
+    s += align256(4 * N1);
+    int32_t* tpad = reinterpret_cast<int32_t*>(s);
     s += align256(4 * N1);
     void* scan_tmp = s;
 
@@ -670,25 +724,18 @@ int gsofa_load_csr(gsofa_ctx* ctx, int32_t n, int64_t nnz, const int32_t* row_be
         if (e != cudaSuccess) { cleanup(); return cuda_fail(ctx, e, #call); } \
     } while (0)
     CKL(cudaMemsetAsync(ctx->small, 0, 128, ctx->stream));
+    CKL(cudaMemcpyAsync(m->rowptr, rp.data(), 4 * N1, cudaMemcpyHostToDevice, ctx->stream));
     if (n > 0) {
-        CKL(cudaMemcpyAsync(dbeg, contiguous ? rowptr.data() : row_begin, 4 * (size_t)n,
-                            cudaMemcpyHostToDevice, ctx->stream));
-        CKL(cudaMemcpyAsync(m->rowptr, rowptr.data(), 4 * N1, cudaMemcpyHostToDevice, ctx->stream));
+        CKL(cudaMemcpyAsync(dbeg, row_begin, 4 * (size_t)n, cudaMemcpyHostToDevice, ctx->stream));
     } else {
-        CKL(cudaMemsetAsync(m->rowptr, 0, 4, ctx->stream));
         CKL(cudaMemsetAsync(m->trowptr, 0, 4, ctx->stream));
     }
-    if (contiguous) {
-        if (packed > 0)
-            CKL(cudaMemcpyAsync(m->col, col, 4 * (size_t)packed, cudaMemcpyHostToDevice, ctx->stream));
-    } else if (nnz > 0) {
+    if (nnz > 0)
         CKL(cudaMemcpyAsync(dcol_in, col, 4 * (size_t)nnz, cudaMemcpyHostToDevice, ctx->stream));
-    }
     CKL(cudaMemsetAsync(tcount, 0, 4 * N1, ctx->stream));
     CKL(cudaMemsetAsync(tfill, 0, 4 * N1, ctx->stream));
-    CKL(launch_canonicalize(n, contiguous ? packed : nnz, dbeg, nullptr, dcol_in, m->rowptr, m->col,
-                            tcount, m->trowptr, m->tcol, tfill, scan_tmp, scan_bytes, dstatus,
-                            ctx->stream));
+    CKL(launch_canonicalize(n, nnz, dbeg, dcol_in, m->rowptr, m->col, tcount, tpad, m->trowptr,
+                            m->tcol, tfill, m->wdeg, scan_tmp, scan_bytes, dstatus, ctx->stream));
     CKL(cudaMemcpyAsync(ctx->h_status, dstatus, 4, cudaMemcpyDeviceToHost, ctx->stream));
     CKL(cudaStreamSynchronize(ctx->stream));
 #undef CKL

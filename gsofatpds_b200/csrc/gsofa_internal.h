@@ -33,6 +33,7 @@ struct MatDesc {
     const int32_t* col;
     const int32_t* trowptr;     // n+1 (A^T)
     const int32_t* tcol;
+    const int32_t* wdeg;        // ceil(n/32): sum of A's row lengths per 32-vertex word
     int32_t* nnz_u;             // n: |U row|
     int32_t* nz_row_u;          // n: reference nz_row_U counter
     uint64_t* dig_u;            // n (or null)
@@ -57,9 +58,17 @@ struct TraverseLaunch {
     int32_t* queue;             // grid * queue_stride ints
     long long queue_stride;
     uint32_t* gbitmap;          // grid * bitmap_words (global-bitmap variant) or null
+    uint32_t* gprev;            // grid * ring * bitmap_words: each CTA's recent closures
+    int chunk;                  // consecutive sources per work item
+    int merge;                  // 1: reuse the closures of reached cached sources
+    int ring;                   // cached closures per CTA (power of 2, <= 32)
     long long bitmap_words;     // words per bitmap (covers max n + padding)
     int32_t* status;            // device error word
     int pattern_pass;           // 1: write patterns instead of counting
+    int bu_alpha;               // top-down -> bottom-up when frontier*alpha > unseen (0: never)
+    int bu_beta;                // bottom-up -> top-down when found*beta < unseen
+    int bu_min_src;             // sources below this id stay top-down
+    int heavy_len;              // padded rows longer than this are walked by a whole warp
 };
 
 // Launch helpers (gsofa_kernels.cu).  All asynchronous on `stream`.
@@ -68,11 +77,13 @@ int traverse_block_sizes(int* sizes, int max_sizes);
 int traverse_occupancy(int block, bool smem_bitmap, size_t smem_bytes);
 cudaError_t launch_traverse(const TraverseLaunch& L, int block, int grid, bool smem_bitmap,
                             size_t smem_bytes, cudaStream_t stream);
-cudaError_t launch_canonicalize(int32_t n, long long nnz, const int32_t* beg, const int32_t* end,
-                                const int32_t* col_in, int32_t* rowptr, int32_t* col_out,
-                                int32_t* tcount, int32_t* trowptr, int32_t* tcol, int32_t* tfill,
-                                void* scan_tmp, size_t scan_tmp_bytes, int32_t* status,
-                                cudaStream_t stream);
+// Builds the padded CSR of A (row pointers rp precomputed on the host, with
+// pad counts in their low 2 bits) and of A^T.
+cudaError_t launch_canonicalize(int32_t n, long long nnz_in, const int32_t* beg,
+                                const int32_t* col_in, const int32_t* rp, int32_t* col_out,
+                                int32_t* tcount, int32_t* tpad, int32_t* trp, int32_t* tcol,
+                                int32_t* tfill, int32_t* wdeg, void* scan_tmp,
+                                size_t scan_tmp_bytes, int32_t* status, cudaStream_t stream);
 size_t canonicalize_scan_bytes(int32_t n);
 cudaError_t launch_supernodes(int32_t n, int32_t mss, const int32_t* nz_row_u,
                               const uint32_t* lmask, int8_t* flags,

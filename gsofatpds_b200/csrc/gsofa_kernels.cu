@@ -9,18 +9,30 @@
 // Here the rule is split in its two halves, each a plain reachability search
 // with a 1-bit "seen" state:
 //   * U row s (m > s): m is adjacent to s or to a vertex reachable from s
-//     through vertices < s.  One BFS from s in A, expanding only ids < s.
+//     through vertices < s.  One search from s in A, expanding only ids < s.
 //   * L column m (s > m): a path s -> m through ids < m is a path m -> s in
-//     A^T through ids < m.  One BFS from m in A^T, expanding only ids < m.
-// Each BFS expands every vertex at most once (no label re-expansions), and
+//     A^T through ids < m.  One search from m in A^T, expanding only ids < m.
+// Each search visits every vertex at most once (no label re-expansions), and
 // its whole state is one bit per vertex, kept in shared memory: n bits =
 // 82 KB at n = 659,033, 125 KB at n = 10^6.
+//
+// A search is direction-optimising (Beamer, Asanovic, Patterson, SC'12):
+// top-down levels expand a frontier queue while it is small; once it is
+// large, bottom-up sweeps test, for every unseen vertex, whether one of its
+// in-neighbours (its row of the other graph) is seen, and a last bottom-up
+// pass marks the ids > source adjacent to the seen set.  Only reachability
+// is needed, so a sweep tests "seen" rather than "in the last frontier".
 //
 // The per-source work item of the reference (one slot of a source group,
 // :2929-3081) becomes a (matrix, source, direction) work item; persistent CTAs
 // take items from a global atomic counter (work stealing), largest sources
 // first.  There is no grid barrier (the reference's barrier.cuh spins) and no
 // wait on another CTA: each CTA only synchronises with itself.
+//
+// Graph layout (both A and A^T): padded CSR.  Row v occupies
+// cl[rp[v] & ~3, rp[v+1] & ~3): a multiple of 4 entries, 16-byte aligned, so
+// rows are read with int4 loads; the last (rp[v+1] & 3) entries repeat v
+// itself, which every test below treats as a no-op.
 #include <cub/block/block_scan.cuh>
 #include <cub/device/device_scan.cuh>
 
@@ -32,7 +44,7 @@ namespace gsofa {
 #define FULL_MASK 0xffffffffu
 
 // Column-set digest term: splitmix64 finaliser (Steele, Lea, Flood 2014).
-__device__ __forceinline__ uint64_t mix64(uint64_t x) {
+__host__ __device__ __forceinline__ uint64_t mix64(uint64_t x) {
     x += 0x9E3779B97F4A7C15ull;
     x = (x ^ (x >> 30)) * 0xBF58476D1CE4E5B9ull;
     x = (x ^ (x >> 27)) * 0x94D049BB133111EBull;
@@ -48,13 +60,29 @@ __device__ __forceinline__ int find_matrix(const MatDesc* mats, int nmats, long 
     return lo;
 }
 
+__device__ __forceinline__ uint32_t ld_vol(const uint32_t* p) {
+    return *reinterpret_cast<const volatile uint32_t*>(p);
+}
+
+__device__ __forceinline__ int4 ld_row4(const int32_t* p) {
+    return __ldg(reinterpret_cast<const int4*>(p));
+}
+
+// Original (unpadded) length of row v of a padded graph.
+__device__ __forceinline__ int row_degree(const int32_t* rp, int v) {
+    const int a = __ldg(rp + v), b = __ldg(rp + v + 1);
+    return (b & ~3) - (a & ~3) - (b & 3);
+}
+
 template <int BLOCK>
 struct TraverseSmem {
     typedef cub::BlockScan<int, BLOCK> Scan;
     typename Scan::TempStorage scan;
-    unsigned long long red[BLOCK / 32][5];
+    unsigned long long red[BLOCK / 32][7];
     long long item;
     int cnt[3];
+    int abort_level;  // set when a cached source is reached: stop, merge, redo
+    int pushed;       // ids a merge appended to the queue
 };
 
 // Bitmap words of a matrix of order n: n bits plus zero padding read by the
@@ -63,15 +91,288 @@ __host__ __device__ __forceinline__ long long bitmap_words_for(int32_t n) {
     return (((long long)n + 31) >> 5) + 6;
 }
 
+struct Src {
+    int32_t src, n;
+    int dir;
+    const int32_t* __restrict__ rp;   // out-graph (top-down)
+    const int32_t* __restrict__ cl;
+    const int32_t* __restrict__ irp;  // in-graph (bottom-up)
+    const int32_t* __restrict__ icl;
+    uint32_t* bm;                     // X: this source's seen bits
+    // The queue and the ring are written and read by different threads of the
+    // CTA across barriers; they are accessed at L2 (.cg) only.
+    // Ring of the closures of the last `ring` sources this CTA finished in the
+    // current chunk: source t lives in slot t & (ring-1).  Sources in
+    // [cache_lo, src) are cached; merged_mask has the slots already merged.
+    const uint32_t* ring_base;
+    long long words;
+    int ring;
+    int32_t cache_lo;
+    uint32_t merged_mask;
+    int top;                          // slot of the largest merged source, -1 if none
+    int* abort_flag;
+};
+
+// The cached source held in ring slot j.
+__device__ __forceinline__ int32_t slot_source(const Src& S, int j) {
+    return S.src - 1 - ((S.src - 1 - j) & (S.ring - 1));
+}
+
+// v lies in R(t) u {t} for the largest merged cached source t (slot `top`):
+// every out-neighbour of v is already in the merged closure, so v needs no
+// expansion.  (Ids in (t, src) of t's closure were only touched by t, never
+// expanded.)  Only an optimisation: a false "no" costs one needless expansion.
+__device__ __forceinline__ bool covered(const Src& S, int top, int32_t v) {
+    if (top < 0 || v > slot_source(S, top)) return false;
+    // plain load: the ring is written by this kernel
+    const uint32_t* y = S.ring_base + (long long)top * S.words;
+    return (__ldcg(y + (v >> 5)) >> (v & 31)) & 1u;
+}
+
+// Slot of the largest source in a merged mask, or -1.
+__device__ __forceinline__ int top_slot(const Src& S, uint32_t mask) {
+    for (int32_t t = S.src - 1; t >= S.cache_lo; t--)
+        if ((mask >> (t & (S.ring - 1))) & 1u) return t & (S.ring - 1);
+    return -1;
+}
+
+// Top-down visit of edge v -> w.  Returns true when w is a new vertex < src
+// to queue.  w == src (also the sentinel of idle lanes and the padding of the
+// source's row) is a no-op.  raw / orig count the source row's entries > src
+// (with multiplicity / distinct) for the reference's nz_row_U counter.
+__device__ __forceinline__ bool td_edge(const Src& S, int v, int w, uint32_t& raw, uint32_t& orig) {
+    if (w == S.src) return false;
+    const uint32_t bit = 1u << (w & 31);
+    uint32_t* word = S.bm + (w >> 5);
+    bool fresh = false;
+    if (!(ld_vol(word) & bit)) fresh = !(atomicOr(word, bit) & bit);
+    if (w > S.src) {
+        if (v == S.src) {
+            raw++;
+            if (fresh) orig++;
+        }
+        return false;
+    }
+    if (fresh && w >= S.cache_lo && !((S.merged_mask >> (w & (S.ring - 1))) & 1u))
+        *(volatile int*)S.abort_flag = 1;
+    return fresh;
+}
+
+// Warp-aggregated append of up to 4 vertices per lane to the queue.
+__device__ __forceinline__ void push4(int32_t* q, long long qcap, long long le, int* cnt,
+                                      int32_t* status, int lane, const int4& e, unsigned f) {
+    const int mine = __popc(f);
+    if (!__any_sync(FULL_MASK, mine)) return;
+    int incl = mine;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int t = __shfl_up_sync(FULL_MASK, incl, o);
+        if (lane >= o) incl += t;
+    }
+    const int total = __shfl_sync(FULL_MASK, incl, 31);
+    int base = 0;
+    if (lane == 31) base = atomicAdd(cnt, total);
+    base = __shfl_sync(FULL_MASK, base, 31);
+    long long at = le + base + (incl - mine);
+    const int ws[4] = {e.x, e.y, e.z, e.w};
+#pragma unroll
+    for (int c = 0; c < 4; c++) {
+        if (f & (1u << c)) {
+            if (at < qcap) __stcg(q + at, ws[c]);
+            else atomicOr(status, DEV_ERR_QUEUE);
+            at++;
+        }
+    }
+}
+
+__device__ __forceinline__ unsigned td_edge4(const Src& S, int v, const int4& e, uint32_t& raw,
+                                             uint32_t& orig) {
+    unsigned f = 0;
+    if (td_edge(S, v, e.x, raw, orig)) f |= 1u;
+    if (td_edge(S, v, e.y, raw, orig)) f |= 2u;
+    if (td_edge(S, v, e.z, raw, orig)) f |= 4u;
+    if (td_edge(S, v, e.w, raw, orig)) f |= 8u;
+    return f;
+}
+
+// One top-down level: expand queue[lb, le), append new vertices after le.
+// After a merge, vertices inside the merged closure (and the source itself)
+// are skipped: their reach is already in the bitmap.
+template <int BLOCK>
+__device__ __forceinline__ void td_level(const Src& S, int32_t* q, long long qcap, long long lb,
+                                         long long le, int* cnt, int32_t* status, int heavy_len,
+                                         uint32_t& raw, uint32_t& orig, uint32_t& trav) {
+    constexpr int NW = BLOCK / 32;
+    const int lane = threadIdx.x & 31;
+    const int warp = threadIdx.x >> 5;
+    const int4 idle = make_int4(S.src, S.src, S.src, S.src);
+    for (long long base = lb + warp * 32; base < le; base += NW * 32) {
+        // stop when a cached source was reached; one value for the whole warp
+        const int ab = __shfl_sync(FULL_MASK, *(volatile int*)S.abort_flag, 0);
+        if (lb > 0 && ab) break;
+        const long long i = base + lane;
+        int v = S.src, s0 = 0, plen = 0;
+        if (i < le) {
+            v = __ldcg(q + i);
+            bool skip = false;
+            if (S.merged_mask) skip = v == S.src || covered(S, S.top, v);
+            if (!skip) {
+                const int r0 = __ldg(S.rp + v), r1 = __ldg(S.rp + v + 1);
+                s0 = r0 & ~3;
+                plen = (r1 & ~3) - s0;
+                trav += (uint32_t)plen;
+            } else {
+                v = S.src;
+            }
+        }
+        // long rows: the whole warp walks one row with coalesced int4 loads
+        unsigned heavy = __ballot_sync(FULL_MASK, plen > heavy_len);
+        while (heavy) {
+            const int l = __ffs(heavy) - 1;
+            heavy &= heavy - 1;
+            const int hb = __shfl_sync(FULL_MASK, s0, l);
+            const int hl = __shfl_sync(FULL_MASK, plen, l);
+            const int hv = __shfl_sync(FULL_MASK, v, l);
+            for (int k0 = 0; k0 < hl; k0 += 128) {
+                const int k = k0 + 4 * lane;
+                const int4 e = k < hl ? ld_row4(S.cl + hb + k) : idle;
+                const unsigned f = td_edge4(S, hv, e, raw, orig);
+                push4(q, qcap, le, cnt, status, lane, e, f);
+            }
+        }
+        if (plen > heavy_len) plen = 0;
+        // short rows: one lane per vertex, 4 entries per int4 load
+        const int its = plen >> 2;
+        const int maxit = __reduce_max_sync(FULL_MASK, its);
+        for (int it = 0; it < maxit; it++) {
+            const int4 e = it < its ? ld_row4(S.cl + s0 + 4 * it) : idle;
+            const unsigned f = td_edge4(S, v, e, raw, orig);
+            push4(q, qcap, le, cnt, status, lane, e, f);
+        }
+    }
+}
+
+__device__ __forceinline__ bool seen_le_src(const Src& S, int p) {
+    return p <= S.src && ((ld_vol(S.bm + (p >> 5)) >> (p & 31)) & 1u);
+}
+
+// Bottom-up sweep.  upper == false: unseen u < src become seen (and queued)
+// when an in-neighbour p <= src is seen.  upper == true: unmarked w in
+// (src, n) are marked when an in-neighbour p <= src is seen.
+template <int BLOCK>
+__device__ __forceinline__ void bu_sweep(const Src& S, bool upper, int32_t* q, long long qcap,
+                                         long long le, int* cnt, int32_t* status, uint32_t& trav) {
+    constexpr int NW = BLOCK / 32;
+    const int lane = threadIdx.x & 31;
+    const int warp = threadIdx.x >> 5;
+    const long long lo = upper ? ((long long)S.src + 1) : 0;
+    const long long hi = upper ? (long long)S.n : (long long)S.src;
+    const long long w0 = lo >> 5, w1 = (hi + 31) >> 5;
+    for (long long wd = w0 + warp; wd < w1; wd += NW) {
+        const long long u = wd * 32 + lane;
+        const bool valid = u >= lo && u < hi;
+        const uint32_t bits = ld_vol(S.bm + wd);
+        const bool need = valid && !((bits >> lane) & 1u);
+        if (!__any_sync(FULL_MASK, need)) continue;
+        bool found = false;
+        if (need) {
+            const int a0 = __ldg(S.irp + u), a1 = __ldg(S.irp + u + 1);
+            const int ib = a0 & ~3, ie = a1 & ~3;
+            for (int j = ib; j < ie; j += 4) {
+                const int4 p = ld_row4(S.icl + j);
+                trav += 4;
+                if (seen_le_src(S, p.x) || seen_le_src(S, p.y) || seen_le_src(S, p.z) ||
+                    seen_le_src(S, p.w)) {
+                    found = true;
+                    break;
+                }
+            }
+        }
+        const unsigned bal = __ballot_sync(FULL_MASK, found);
+        if (!bal) continue;
+        const int leader = __ffs(bal) - 1;
+        if (lane == leader) atomicOr(S.bm + wd, bal);
+        if (!upper) {
+            int base = 0;
+            if (lane == leader) base = atomicAdd(cnt, __popc(bal));
+            base = __shfl_sync(FULL_MASK, base, leader);
+            if (found) {
+                const long long at = le + base + __popc(bal & ((1u << lane) - 1u));
+                if (at < qcap) __stcg(q + at, (int32_t)u);
+                else atomicOr(status, DEV_ERR_QUEUE);
+            }
+        }
+    }
+}
+
+// Merges the closures of the cached sources that the search has reached.
+// If t in [cache_lo, src) is reached then t's closure (its R(t), t and its
+// entries > t) belongs to src's closure.  Reached sources are taken from the
+// largest down; one inside an already merged R(t') u {t'} adds nothing.
+// Vertices of (t, src) that only the merge set were never expanded: they are
+// appended to the queue at `at` (*pushed gets their number).  Block-wide,
+// uniform; returns the new merged mask.
+template <int BLOCK>
+__device__ __forceinline__ uint32_t merge_reached(const Src& S, uint32_t* bm, int32_t* q,
+                                                  long long at, long long qcap, int* pushed,
+                                                  int32_t* status, bool& did_merge) {
+    uint32_t add = 0;
+    did_merge = false;
+    uint32_t mm = S.merged_mask;
+    for (int32_t t = S.src - 1; t >= S.cache_lo; t--) {
+        const int slot = t & (S.ring - 1);
+        if ((mm >> slot) & 1u) continue;
+        if (!((ld_vol(bm + (t >> 5)) >> (t & 31)) & 1u)) continue;
+        const bool inside = covered(S, top_slot(S, mm), t);
+        mm |= 1u << slot;
+        if (!inside) add |= 1u << slot;
+    }
+    // window [cache_lo, src) spans at most 32 ids: two words before the merge
+    const long long w0 = S.cache_lo >> 5, w1 = (S.src - 1) >> 5;
+    const uint32_t b0 = ld_vol(bm + w0), b1 = ld_vol(bm + w1);
+    // Every thread must finish reading the bitmap before any thread goes on:
+    // without this barrier a fast thread that found nothing to merge starts
+    // the next level and sets bits a slow thread is still reading, the slow
+    // thread then decides differently and the block's barriers fall out of
+    // step.
+    __syncthreads();
+    if (!add) return mm;
+    did_merge = true;
+    for (long long i = threadIdx.x; i < S.words; i += BLOCK) {
+        uint32_t x = bm[i];
+        for (uint32_t a = add; a; a &= a - 1)
+            x |= __ldcg(S.ring_base + (long long)(__ffs(a) - 1) * S.words + i);
+        bm[i] = x;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int np = 0;
+        const int top = top_slot(S, mm);
+        for (int32_t v = S.cache_lo; v < S.src; v++) {
+            const long long w = v >> 5;
+            const uint32_t before = w == w0 ? b0 : b1;
+            const uint32_t bit = 1u << (v & 31);
+            if ((before & bit) || !(ld_vol(bm + w) & bit)) continue;  // not set by the merge
+            if (covered(S, top, v)) continue;
+            if (at + np < qcap) __stcg(q + at + np, v);
+            else atomicOr(status, DEV_ERR_QUEUE);
+            np++;
+        }
+        *pushed = np;
+    }
+    return mm;
+}
+
 template <int BLOCK, bool SMEM_BM>
-__global__ void __launch_bounds__(BLOCK) traverse_kernel(TraverseLaunch P) {
+__global__ void __launch_bounds__(BLOCK, 1024 / BLOCK) traverse_kernel(TraverseLaunch P) {
     extern __shared__ uint4 dyn_smem[];
-    __shared__ TraverseSmem<BLOCK> S;
+    __shared__ TraverseSmem<BLOCK> SM;
     constexpr int NW = BLOCK / 32;
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
     uint32_t* bm = SMEM_BM ? reinterpret_cast<uint32_t*>(dyn_smem)
                            : P.gbitmap + (long long)blockIdx.x * P.bitmap_words;
+    uint32_t* ring_base = P.gprev + (long long)blockIdx.x * P.ring * P.bitmap_words;
     int32_t* q = P.queue + (long long)blockIdx.x * P.queue_stride;
     const long long qcap = P.queue_stride;
 
@@ -79,143 +380,235 @@ __global__ void __launch_bounds__(BLOCK) traverse_kernel(TraverseLaunch P) {
 
     // thread 0 accumulates per-matrix counters and flushes on matrix change
     int acc_mat = -1;
-    unsigned long long acc[7] = {0, 0, 0, 0, 0, 0, 0};
+    unsigned long long acc[6] = {0, 0, 0, 0, 0, 0};
 
     for (;;) {
-        if (threadIdx.x == 0) S.item = (long long)atomicAdd(P.work_counter, 1ull);
+        if (threadIdx.x == 0) SM.item = (long long)atomicAdd(P.work_counter, 1ull);
         __syncthreads();
-        const long long item = S.item;
+        const long long item = SM.item;
         if (item >= P.total_items) break;
         const int mi = find_matrix(P.mats, P.nmats, item);
         const MatDesc& M = P.mats[mi];
         const int32_t n = M.n;
         const long long local = item - M.item_base;
-        const int32_t src = n - 1 - (int32_t)(local >> 1);
         const int dir = (int)(local & 1);
-        const int32_t* __restrict__ rp = dir ? M.trowptr : M.rowptr;
-        const int32_t* __restrict__ cl = dir ? M.tcol : M.col;
-        const bool scatter = dir == 1 && M.nnz_lr != nullptr && !P.pattern_pass;
+        const long long nchunks = ((long long)n + P.chunk - 1) / P.chunk;
+        const long long chunk = nchunks - 1 - (local >> 1);  // largest sources first
+        const int32_t s_first = (int32_t)(chunk * P.chunk);
+        const int32_t s_end = (int32_t)min((long long)n, (chunk + 1) * P.chunk);
+        const long long words = bitmap_words_for(n);
+        const long long nwords = ((long long)n + 31) >> 5;
+
+        Src S;
+        S.n = n;
+        S.dir = dir;
+        S.rp = dir ? M.trowptr : M.rowptr;
+        S.cl = dir ? M.tcol : M.col;
+        S.irp = dir ? M.rowptr : M.trowptr;
+        S.icl = dir ? M.col : M.tcol;
+        S.bm = bm;
+        S.ring_base = ring_base;
+        S.words = P.bitmap_words;
+        S.ring = P.ring;
+        S.abort_flag = &SM.abort_level;
         const bool digests = M.dig_u != nullptr;
+        const bool scatter = dir == 1 && M.nnz_lr != nullptr && !P.pattern_pass;
 
-        if (threadIdx.x == 0) {
-            bm[src >> 5] |= 1u << (src & 31);
-            q[0] = src;
-            S.cnt[0] = 0;
-        }
-        __syncthreads();
+        for (int32_t src = s_first; src < s_end; src++) {
+            S.src = src;
+            // cached: the last `ring` sources of this chunk (none without merging)
+            S.cache_lo = P.merge ? max(s_first, src - P.ring) : src;
+            S.merged_mask = 0u;
+            S.top = -1;
+            if (threadIdx.x == 0) {
+                bm[src >> 5] |= 1u << (src & 31);
+                __stcg(q, src);
+                SM.cnt[0] = 0;
+                SM.abort_level = 0;
+            }
+            __syncthreads();
 
-        unsigned long long t_gt = 0, t_orig = 0, t_raw = 0, t_edges = 0, t_dig = 0;
-        long long lb = 0, le = 1;
-        int level = 0;
-        while (lb < le) {
-            if (threadIdx.x == 0) S.cnt[(level + 1) % 3] = 0;
-            int* cnt = &S.cnt[level % 3];
-            for (long long base = lb + warp * 32; base < le; base += NW * 32) {
-                const long long i = base + lane;
-                int v = -1, b = 0, deg = 0;
-                if (i < le) {
-                    v = q[i];
-                    b = rp[v];
-                    deg = rp[v + 1] - b;
-                }
-                t_edges += (unsigned long long)deg;
-                int incl = deg;
-#pragma unroll
-                for (int o = 1; o < 32; o <<= 1) {
-                    int t = __shfl_up_sync(FULL_MASK, incl, o);
-                    if (lane >= o) incl += t;
-                }
-                const int total = __shfl_sync(FULL_MASK, incl, 31);
-                const int excl = incl - deg;
-                for (int k0 = 0; k0 < total; k0 += 32) {
-                    const int k = k0 + lane;
-                    // owner lane: the last lane whose exclusive offset <= k
-                    int lo = 0;
-#pragma unroll
-                    for (int st = 16; st > 0; st >>= 1) {
-                        int c = lo + st;
-                        int ex = __shfl_sync(FULL_MASK, excl, c);
-                        if (ex <= k) lo = c;
+            uint32_t raw = 0, orig = 0, trav = 0;
+            long long lb = 0, le = 1;
+            int level = 0;
+            bool bottom_up = false, used_bu = false;
+            const bool allow_bu = P.bu_alpha > 0 && src >= P.bu_min_src;
+            for (;;) {
+                if (!bottom_up) {
+                    if (lb >= le) break;
+                    const long long unseen = (long long)src - (le - 1);
+                    if (allow_bu && lb > 0 && (le - lb) * (long long)P.bu_alpha > unseen) {
+                        bottom_up = used_bu = true;
+                        continue;
                     }
-                    const int ob = __shfl_sync(FULL_MASK, b, lo);
-                    const int oex = __shfl_sync(FULL_MASK, excl, lo);
-                    const int ov = __shfl_sync(FULL_MASK, v, lo);
-                    bool push = false;
-                    int w = -1;
-                    if (k < total) {
-                        w = cl[ob + (k - oex)];
-                        if (w != src) {
-                            const uint32_t bit = 1u << (w & 31);
-                            uint32_t* word = bm + (w >> 5);
-                            bool fresh = false;
-                            if (!(*(volatile uint32_t*)word & bit))
-                                fresh = !(atomicOr(word, bit) & bit);
-                            if (w > src) {
-                                if (ov == src) t_raw++;
-                                if (fresh) {
-                                    t_gt++;
-                                    if (ov == src) t_orig++;
-                                    if (digests) t_dig += mix64((uint64_t)w);
-                                    if (scatter) {
-                                        atomicAdd(&M.nnz_lr[w], 1);
-                                        atomicAdd((unsigned long long*)&M.dig_lr[w],
-                                                  (unsigned long long)mix64((uint64_t)src));
-                                    }
-                                }
-                            } else if (fresh) {
-                                push = true;
-                            }
+                    if (threadIdx.x == 0) SM.cnt[(level + 1) % 3] = 0;
+                    td_level<BLOCK>(S, q, qcap, lb, le, &SM.cnt[level % 3], P.status, P.heavy_len,
+                                    raw, orig, trav);
+                    __syncthreads();
+                    const int nxt = SM.cnt[level % 3];
+                    level++;
+                    // a reached cached source's closure is ours: merge it
+                    bool did = false;
+                    const uint32_t mm =
+                        S.cache_lo < src ? merge_reached<BLOCK>(S, bm, q, le + nxt, qcap, &SM.pushed,
+                                                                P.status, did)
+                                         : S.merged_mask;
+                    if (mm != S.merged_mask) {
+                        S.merged_mask = mm;
+                        S.top = top_slot(S, mm);
+                        if (threadIdx.x == 0) SM.abort_level = 0;
+                        __syncthreads();
+                        const int np = did ? SM.pushed : 0;
+                        le = le + nxt + np;  // redo this level (it may have been cut short)
+                    } else {
+                        lb = le;
+                        le = le + nxt;
+                    }
+                    if (le > qcap) le = qcap;  // unreachable: each vertex is queued once
+                } else {
+                    const long long unseen = (long long)src - (le - 1);
+                    if (threadIdx.x == 0) SM.cnt[(level + 1) % 3] = 0;
+                    bu_sweep<BLOCK>(S, false, q, qcap, le, &SM.cnt[level % 3], P.status, trav);
+                    __syncthreads();
+                    const int found = SM.cnt[level % 3];
+                    level++;
+                    lb = le;
+                    le = le + found;
+                    if (le > qcap) le = qcap;
+                    bool did = false;
+                    const uint32_t mm =
+                        S.cache_lo < src ? merge_reached<BLOCK>(S, bm, q, le, qcap, &SM.pushed,
+                                                                P.status, did)
+                                         : S.merged_mask;
+                    if (mm != S.merged_mask) {
+                        S.merged_mask = mm;
+                        S.top = top_slot(S, mm);
+                        if (threadIdx.x == 0) SM.abort_level = 0;
+                        __syncthreads();
+                        le = le + (did ? SM.pushed : 0);  // merged-in ids become queue entries
+                        continue;  // sweep again with the merged closure
+                    }
+                    if (found == 0) break;
+                    if ((long long)found * P.bu_beta < unseen) bottom_up = false;  // few new
+                }
+            }
+            if (used_bu) {
+                bu_sweep<BLOCK>(S, true, q, qcap, le, nullptr, P.status, trav);
+                __syncthreads();
+            }
+
+            if (dir == 1 && !P.pattern_pass && threadIdx.x < 4) {
+                // 128-bit mask of rows f+1 .. f+128 in L column f (supernode test)
+                const long long p = (long long)src + 1 + 32 * threadIdx.x;
+                const long long wd = p >> 5;
+                const int off = (int)(p & 31);
+                uint32_t val = bm[wd] >> off;
+                if (off) val |= bm[wd + 1] << (32 - off);
+                M.lmask[4ll * src + threadIdx.x] = val;
+            }
+            if (P.pattern_pass) {
+                // sorted ids of the set bits > src: U row (dir 0) or L column (dir 1)
+                int32_t* out = dir == 0 ? M.ucols : M.lrows;
+                const long long obase = dir == 0 ? M.uptr[src] : M.lptr[src];
+                long long wpos = ((long long)src + 1) >> 5;
+                long long written = 0;
+                for (; wpos < nwords; wpos += BLOCK) {
+                    const long long wi = wpos + threadIdx.x;
+                    uint32_t word = 0;
+                    if (wi < nwords) {
+                        word = bm[wi];
+                        const long long first = wi << 5;
+                        if (first <= src) {  // drop bits <= src
+                            const int keep_from = (int)(src - first) + 1;
+                            word = keep_from >= 32 ? 0u : (word & (~0u << keep_from));
                         }
                     }
-                    const unsigned bal = __ballot_sync(FULL_MASK, push);
-                    if (bal) {
-                        const int leader = __ffs(bal) - 1;
-                        int pos = 0;
-                        if (lane == leader) pos = atomicAdd(cnt, __popc(bal));
-                        pos = __shfl_sync(FULL_MASK, pos, leader);
-                        if (push) {
-                            const long long at = le + pos + __popc(bal & ((1u << lane) - 1u));
-                            if (at < qcap) q[at] = w;
-                            else atomicOr(P.status, DEV_ERR_QUEUE);
+                    int cntw = __popc(word), ex = 0, tot = 0;
+                    typename TraverseSmem<BLOCK>::Scan(SM.scan).ExclusiveSum(cntw, ex, tot);
+                    long long o = obase + written + ex;
+                    while (word) {
+                        const int bpos = __ffs(word) - 1;
+                        word &= word - 1;
+                        out[o++] = (int32_t)((wi << 5) + bpos);
+                    }
+                    written += tot;
+                    __syncthreads();  // scan storage reuse
+                }
+            }
+            __syncthreads();
+
+            // ---- census of the closure: counts and digests from the bitmap; the
+            // bitmap moves to the CTA's previous-closure buffer and is cleared
+            unsigned long long c_gt = 0, c_v = 0, c_e = 0, c_dig = 0;
+            const bool keep = P.merge && src + 1 < s_end;
+            uint32_t* keep_slot = ring_base + (long long)(src & (P.ring - 1)) * P.bitmap_words;
+            for (long long w = threadIdx.x; w < words; w += BLOCK) {
+                const uint32_t x = bm[w];
+                bm[w] = 0u;
+                if (keep) __stcg(keep_slot + w, x);
+                if (!x || w >= nwords) continue;
+                const long long base = w << 5;
+                uint32_t lo_m, hi_m;
+                if (base + 31 < src) { lo_m = ~0u; hi_m = 0u; }
+                else if (base > src) { lo_m = 0u; hi_m = ~0u; }
+                else {
+                    const int b = (int)(src - base);  // 0..31: bit of src
+                    lo_m = b ? ((1u << b) - 1u) : 0u;
+                    hi_m = b == 31 ? 0u : (~0u << (b + 1));
+                }
+                const uint32_t xl = x & lo_m, xh = x & hi_m;
+                c_v += __popc(xl);
+                if (dir == 0 && xl) {
+                    if (xl == ~0u) {
+                        c_e += (unsigned long long)__ldg(M.wdeg + w);
+                    } else {
+                        uint32_t t = xl;
+                        while (t) {
+                            const int bp = __ffs(t) - 1;
+                            t &= t - 1;
+                            c_e += (unsigned long long)row_degree(M.rowptr, (int)(base + bp));
+                        }
+                    }
+                }
+                c_gt += __popc(xh);
+                if ((digests || scatter) && xh) {
+                    uint32_t t = xh;
+                    while (t) {
+                        const int bp = __ffs(t) - 1;
+                        t &= t - 1;
+                        const int wv = (int)(base + bp);
+                        if (digests) c_dig += mix64((uint64_t)wv);
+                        if (scatter) {
+                            atomicAdd(&M.nnz_lr[wv], 1);
+                            atomicAdd((unsigned long long*)&M.dig_lr[wv],
+                                      (unsigned long long)mix64((uint64_t)src));
                         }
                     }
                 }
             }
+            unsigned long long vals[7] = {c_gt, raw, orig, c_v, c_e, c_dig, trav};
+#pragma unroll
+            for (int j = 0; j < 7; j++) {
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) vals[j] += __shfl_xor_sync(FULL_MASK, vals[j], o);
+            }
+            if (lane == 0) {
+#pragma unroll
+                for (int j = 0; j < 7; j++) SM.red[warp][j] = vals[j];
+            }
             __syncthreads();
-            const int nxt = *cnt;
-            lb = le;
-            le = le + nxt;
-            if (le > qcap) le = qcap;  // unreachable: at most n vertices are queued
-            level++;
-        }
-
-        // ---- per-source reduction
-        unsigned long long vals[5] = {t_gt, t_orig, t_raw, t_edges, t_dig};
-#pragma unroll
-        for (int j = 0; j < 5; j++) {
-#pragma unroll
-            for (int o = 16; o > 0; o >>= 1) vals[j] += __shfl_xor_sync(FULL_MASK, vals[j], o);
-        }
-        if (lane == 0) {
-#pragma unroll
-            for (int j = 0; j < 5; j++) S.red[warp][j] = vals[j];
-        }
-        __syncthreads();
-        if (threadIdx.x == 0) {
-            unsigned long long r[5] = {0, 0, 0, 0, 0};
-            for (int wi = 0; wi < NW; wi++)
-                for (int j = 0; j < 5; j++) r[j] += S.red[wi][j];
-            const unsigned long long gt = r[0], orig = r[1], raw = r[2], edges = r[3];
-            const unsigned long long dig = r[4];
-            const long long src_deg = (long long)rp[src + 1] - rp[src];
-            if (!P.pattern_pass) {
+            if (threadIdx.x == 0 && !P.pattern_pass) {
+                unsigned long long r[7] = {0, 0, 0, 0, 0, 0, 0};
+                for (int wi = 0; wi < NW; wi++)
+                    for (int j = 0; j < 7; j++) r[j] += SM.red[wi][j];
+                const unsigned long long gt = r[0], rw = r[1], og = r[2], vv = r[3], ee = r[4];
                 if (dir == 0) {
                     M.nnz_u[src] = (int32_t)gt;
-                    M.nz_row_u[src] = (int32_t)(raw + gt - orig);
-                    if (digests) M.dig_u[src] = dig;
+                    M.nz_row_u[src] = (int32_t)(rw + gt - og);
+                    if (digests) M.dig_u[src] = r[5];
                 } else {
                     M.nnz_lc[src] = (int32_t)gt;
-                    if (digests) M.dig_lc[src] = dig;
+                    if (digests) M.dig_lc[src] = r[5];
                 }
                 if (acc_mat != mi) {
                     if (acc_mat >= 0) {
@@ -228,62 +621,20 @@ __global__ void __launch_bounds__(BLOCK) traverse_kernel(TraverseLaunch P) {
                         atomicAdd(&c[CNT_NNZ_L], acc[5]);
                     }
                     acc_mat = mi;
-                    for (int j = 0; j < 7; j++) acc[j] = 0;
+                    for (int j = 0; j < 6; j++) acc[j] = 0;
                 }
-                acc[0] += gt - orig;
-                acc[3] += edges;
+                acc[0] += gt - og;
+                acc[3] += r[6];
                 if (dir == 0) {
-                    acc[1] += edges - (unsigned long long)src_deg;
-                    acc[2] += (unsigned long long)(le - 1);
+                    acc[1] += ee;
+                    acc[2] += vv;
                     acc[4] += gt;
                 } else {
                     acc[5] += gt;
                 }
             }
+            __syncthreads();
         }
-        if (dir == 1 && !P.pattern_pass && threadIdx.x < 4) {
-            // 128-bit mask of rows f+1 .. f+128 in L column f (supernode test)
-            const long long p = (long long)src + 1 + 32 * threadIdx.x;
-            const long long wd = p >> 5;
-            const int off = (int)(p & 31);
-            uint32_t val = bm[wd] >> off;
-            if (off) val |= bm[wd + 1] << (32 - off);
-            M.lmask[4ll * src + threadIdx.x] = val;
-        }
-        if (P.pattern_pass) {
-            // sorted ids of the set bits > src: U row (dir 0) or L column (dir 1)
-            int32_t* out = dir == 0 ? M.ucols : M.lrows;
-            const long long obase = dir == 0 ? M.uptr[src] : M.lptr[src];
-            const long long nw = ((long long)n + 31) >> 5;
-            long long wpos = ((long long)src + 1) >> 5;
-            long long written = 0;
-            for (; wpos < nw; wpos += BLOCK) {
-                const long long wi = wpos + threadIdx.x;
-                uint32_t word = 0;
-                if (wi < nw) {
-                    word = bm[wi];
-                    const long long first = wi << 5;
-                    if (first <= src) {  // drop bits <= src
-                        const int keep_from = (int)(src - first) + 1;
-                        word = keep_from >= 32 ? 0u : (word & (~0u << keep_from));
-                    }
-                }
-                int cntw = __popc(word), ex = 0, tot = 0;
-                typename TraverseSmem<BLOCK>::Scan(S.scan).ExclusiveSum(cntw, ex, tot);
-                long long o = obase + written + ex;
-                while (word) {
-                    const int bpos = __ffs(word) - 1;
-                    word &= word - 1;
-                    out[o++] = (int32_t)((wi << 5) + bpos);
-                }
-                written += tot;
-                __syncthreads();  // scan storage reuse
-            }
-        }
-        __syncthreads();
-        const long long words = bitmap_words_for(n);
-        for (long long i = threadIdx.x; i < words; i += BLOCK) bm[i] = 0u;
-        __syncthreads();
     }
     if (threadIdx.x == 0 && acc_mat >= 0) {
         unsigned long long* c = P.mats[acc_mat].counters;
@@ -358,11 +709,14 @@ cudaError_t launch_traverse(const TraverseLaunch& L, int block, int grid, bool s
 #undef LAUNCH_CASE
 }
 
-// ---- ingest: gather rows into contiguous CSR and build A^T ------------------
+// ---- ingest: padded CSR of A and of A^T --------------------------------------
+//
+// The host computes A's padded row pointers (pad counts in the low 2 bits).
+// One warp per row copies the row into its padded slot, writes the padding
+// (the row's own id) and counts the entries per column for A^T.
 
-// One warp per row: copy the row's entries and count them per column.
 __global__ void gather_rows_kernel(int32_t n, long long nnz_in, const int32_t* __restrict__ beg,
-                                   const int32_t* __restrict__ rowptr,
+                                   const int32_t* __restrict__ rp,
                                    const int32_t* __restrict__ col_in, int32_t* __restrict__ col_out,
                                    int32_t* __restrict__ tcount, int32_t* status) {
     const long long gw = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -370,18 +724,28 @@ __global__ void gather_rows_kernel(int32_t n, long long nnz_in, const int32_t* _
     const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
     for (long long v = gw; v < n; v += nwarps) {
         const long long b = beg[v];
-        const long long o = rowptr[v];
-        const long long d = (long long)rowptr[v + 1] - o;
-        for (long long j = lane; j < d; j += 32) {
+        const int r0 = rp[v], r1 = rp[v + 1];
+        const long long o = r0 & ~3;
+        const long long plen = (long long)(r1 & ~3) - o;
+        const long long d = plen - (r1 & 3);
+        for (long long j = lane; j < plen; j += 32) {
+            if (j >= d) {
+                col_out[o + j] = (int32_t)v;
+                continue;
+            }
             const long long src = b + j;
+            // invalid entries become self loops so A^T stays consistent; the
+            // status word makes the load fail afterwards
             if (src < 0 || src >= nnz_in) {
                 atomicOr(status, DEV_ERR_ROW_RANGE);
+                col_out[o + j] = (int32_t)v;
+                atomicAdd(&tcount[v], 1);
                 continue;
             }
             const int32_t c = col_in[src];
             if (c < 0 || c >= n) {
                 atomicOr(status, DEV_ERR_COL_RANGE);
-                col_out[o + j] = (int32_t)v;  // keep the structure in range
+                col_out[o + j] = (int32_t)v;
                 atomicAdd(&tcount[v], 1);
                 continue;
             }
@@ -391,20 +755,66 @@ __global__ void gather_rows_kernel(int32_t n, long long nnz_in, const int32_t* _
     }
 }
 
-__global__ void transpose_scatter_kernel(int32_t n, const int32_t* __restrict__ rowptr,
+// tpad[c] = count rounded up to a multiple of 4 (tpad[n] = 0 for the scan).
+__global__ void pad_counts_kernel(int32_t n, const int32_t* __restrict__ tcount,
+                                  int32_t* __restrict__ tpad) {
+    for (long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x; c <= n;
+         c += (long long)gridDim.x * blockDim.x)
+        tpad[c] = c < n ? ((tcount[c] + 3) & ~3) : 0;
+}
+
+// After the exclusive scan of tpad into trp: store each row's pad count in
+// the low bits of the next row pointer.
+__global__ void encode_pads_kernel(int32_t n, const int32_t* __restrict__ tcount,
+                                   const int32_t* __restrict__ tpad, int32_t* __restrict__ trp) {
+    for (long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x; c < n;
+         c += (long long)gridDim.x * blockDim.x)
+        trp[c + 1] |= tpad[c] - tcount[c];
+}
+
+__global__ void transpose_scatter_kernel(int32_t n, const int32_t* __restrict__ rp,
                                          const int32_t* __restrict__ col,
-                                         const int32_t* __restrict__ trowptr,
+                                         const int32_t* __restrict__ trp,
                                          int32_t* __restrict__ tfill, int32_t* __restrict__ tcol) {
     const long long gw = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31;
     const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
     for (long long v = gw; v < n; v += nwarps) {
-        const int b = rowptr[v], e = rowptr[v + 1];
+        const int r0 = rp[v], r1 = rp[v + 1];
+        const int b = r0 & ~3, e = (r1 & ~3) - (r1 & 3);
         for (int j = b + lane; j < e; j += 32) {
             const int c = col[j];
             const int pos = atomicAdd(&tfill[c], 1);
-            tcol[trowptr[c] + pos] = (int32_t)v;
+            tcol[(trp[c] & ~3) + pos] = (int32_t)v;
         }
+    }
+}
+
+// wdeg[w] = total length of A's rows 32w .. 32w+31 (census of full words).
+__global__ void word_degree_kernel(int32_t n, const int32_t* __restrict__ rp,
+                                   int32_t* __restrict__ wdeg) {
+    const long long nw = ((long long)n + 31) >> 5;
+    const int lane = threadIdx.x & 31;
+    const long long gw = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    for (long long w = gw; w < nw; w += ((long long)gridDim.x * blockDim.x) >> 5) {
+        const long long v = (w << 5) + lane;
+        int d = 0;
+        if (v < n) {
+            const int r0 = rp[v], r1 = rp[v + 1];
+            d = (r1 & ~3) - (r0 & ~3) - (r1 & 3);
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) d += __shfl_xor_sync(FULL_MASK, d, o);
+        if (lane == 0) wdeg[w] = d;
+    }
+}
+
+__global__ void transpose_pad_kernel(int32_t n, const int32_t* __restrict__ tcount,
+                                     const int32_t* __restrict__ trp, int32_t* __restrict__ tcol) {
+    for (long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x; c < n;
+         c += (long long)gridDim.x * blockDim.x) {
+        const int b = trp[c] & ~3, e = trp[c + 1] & ~3;
+        for (int j = b + tcount[c]; j < e; j++) tcol[j] = (int32_t)c;
     }
 }
 
@@ -415,27 +825,34 @@ size_t canonicalize_scan_bytes(int32_t n) {
     return bytes;
 }
 
-// rowptr (n+1) is already on the device (computed on the host from beg/end).
-// tcount and tfill: n+1 zeroed ints.  col_in may equal col_out when the rows
-// are already contiguous in order (then only validation + counting happens).
-cudaError_t launch_canonicalize(int32_t n, long long nnz_in, const int32_t* beg, const int32_t* /*end*/,
-                                const int32_t* col_in, int32_t* rowptr, int32_t* col_out,
-                                int32_t* tcount, int32_t* trowptr, int32_t* tcol, int32_t* tfill,
-                                void* scan_tmp, size_t scan_tmp_bytes, int32_t* status,
-                                cudaStream_t st) {
+// rp (A, n+1, encoded) is on the device.  tcount/tfill/tpad: n+1 zeroed ints.
+// col_in may equal col_out only when no row moves and no row is padded.
+cudaError_t launch_canonicalize(int32_t n, long long nnz_in, const int32_t* beg,
+                                const int32_t* col_in, const int32_t* rp, int32_t* col_out,
+                                int32_t* tcount, int32_t* tpad, int32_t* trp, int32_t* tcol,
+                                int32_t* tfill, int32_t* wdeg, void* scan_tmp,
+                                size_t scan_tmp_bytes, int32_t* status, cudaStream_t st) {
     if (n <= 0) return cudaSuccess;
     const int threads = 256;
-    long long warps_needed = n;
-    int grid = (int)((warps_needed * 32 + threads - 1) / threads);
-    if (grid > 148 * 64) grid = 148 * 64;
-    gather_rows_kernel<<<grid, threads, 0, st>>>(n, nnz_in, beg, rowptr, col_in, col_out, tcount,
-                                                 status);
+    long long grid_w = ((long long)n * 32 + threads - 1) / threads;
+    int grid = (int)(grid_w > 148 * 64 ? 148 * 64 : grid_w);
+    long long grid_t = ((long long)n + threads) / threads;
+    int gridt = (int)(grid_t > 148 * 16 ? 148 * 16 : grid_t);
+    gather_rows_kernel<<<grid, threads, 0, st>>>(n, nnz_in, beg, rp, col_in, col_out, tcount, status);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
+    pad_counts_kernel<<<gridt, threads, 0, st>>>(n, tcount, tpad);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
     size_t bytes = scan_tmp_bytes;
-    e = cub::DeviceScan::ExclusiveSum(scan_tmp, bytes, tcount, trowptr, (int)n + 1, st);
+    e = cub::DeviceScan::ExclusiveSum(scan_tmp, bytes, tpad, trp, (int)n + 1, st);
     if (e != cudaSuccess) return e;
-    transpose_scatter_kernel<<<grid, threads, 0, st>>>(n, rowptr, col_out, trowptr, tfill, tcol);
+    encode_pads_kernel<<<gridt, threads, 0, st>>>(n, tcount, tpad, trp);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    transpose_scatter_kernel<<<grid, threads, 0, st>>>(n, rp, col_out, trp, tfill, tcol);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    transpose_pad_kernel<<<gridt, threads, 0, st>>>(n, tcount, trp, tcol);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    word_degree_kernel<<<gridt, threads, 0, st>>>(n, rp, wdeg);
     return cudaGetLastError();
 }
 

@@ -46,6 +46,9 @@ typedef struct gsofa_result gsofa_result;
 /* Diagnostic: keep the traversal's seen-bitmap in global memory even when
  * it fits in shared memory (the variant used for orders above ~1.8M). */
 #define GSOFA_FORCE_GLOBAL_BITMAP (1u << 30)
+/* Diagnostic: never reuse the previous source's closure (every source is
+ * searched from scratch). */
+#define GSOFA_NO_MERGE (1u << 29)
 
 typedef struct gsofa_opts {
     /* rows per supernode chunk; the reference's max_supernode_size, argv[5]
@@ -58,6 +61,24 @@ typedef struct gsofa_opts {
      * The reference's N_src_group (Compute_Src_group, :1031-1048) */
     int32_t sources_in_flight;
     uint32_t flags; /* GSOFA_* option bits */
+    /* traversal direction switch: a search turns from top-down to bottom-up
+     * sweeps when frontier * bu_alpha exceeds its unseen vertices, and back
+     * when a sweep finds fewer than unseen / bu_beta; 0 = defaults,
+     * bu_alpha < 0 = top-down only */
+    int32_t bu_alpha;
+    int32_t bu_beta;
+    /* rows longer than this many entries are walked by a whole warp instead
+     * of one lane; 0 = default */
+    int32_t heavy_row;
+    /* sources with a smaller id always stay top-down; 0 = default (2048) */
+    int32_t bu_min_source;
+    /* consecutive sources one CTA takes as a work item (the previous source's
+     * closure is reused inside a chunk); 0 = default */
+    int32_t chunk_sources;
+    /* closures of recently finished sources each CTA keeps for reuse
+     * (rounded down to a power of 2, at most 32); 0 = default */
+    int32_t cached_closures;
+    int32_t reserved[2];
 } gsofa_opts;
 
 /* Defaults: max_supernode_size 128, autotuned CTA size, GPU-filling

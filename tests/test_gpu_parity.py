@@ -72,14 +72,30 @@ def check_full(res, r, rt, mss=128, l_rows=True, supernodes=True):
         assert c["n_supernodes"] == nsup + 1
 
 
-def test_bc_matches_reference_and_oracle(ctx):
+# traversal modes: defaults; bottom-up as early as possible with warp-walked
+# rows from 4 entries, 7-source chunks and 2 cached closures; top-down only
+# without closure reuse; bottom-up without switching back, 1000-source chunks
+# and 32 cached closures
+MODES = [dict(), dict(bu_alpha=1000, bu_min_source=1, heavy_row=4, chunk_sources=7,
+                     cached_closures=2),
+         dict(bu_alpha=-1, heavy_row=8, merge=False),
+         dict(bu_alpha=2, bu_beta=1, bu_min_source=1, chunk_sources=1000, cached_closures=32)]
+
+
+@pytest.fixture(scope="module")
+def bc_oracle():
     z = load_bc()
+    return z, oracle_full(z["beg"], z["end"], z["col"], pattern=True)
+
+
+@pytest.mark.parametrize("mode", range(4))
+def test_bc_matches_reference_and_oracle(ctx, bc_oracle, mode):
+    z, (r, rt) = bc_oracle
     m = ctx.load_csr(z["beg"], z["end"], z["col"])  # non-contiguous, unsorted rows
-    res = ctx.factor(m, l_row_stats=True, pattern=True)
+    res = ctx.factor(m, l_row_stats=True, pattern=True, **MODES[mode])
     c = res.counts
     assert c["fill_count"] == 980136  # reference log, with_supernodes/...warp_centric.dat:2
     assert c["n_supernodes"] == 6800
-    r, rt = oracle_full(z["beg"], z["end"], z["col"], pattern=True)
     check_full(res, r, rt)
     up, uc = res.pattern_u()
     np.testing.assert_array_equal(up, r["Uptr"])
@@ -91,7 +107,7 @@ def test_bc_matches_reference_and_oracle(ctx):
     m.close()
 
 
-@pytest.mark.parametrize("seed", range(10))
+@pytest.mark.parametrize("seed", range(12))
 def test_random_small_patterns(ctx, seed):
     rng = np.random.default_rng(100 + seed)
     n = int(rng.integers(1, 300))
@@ -102,7 +118,7 @@ def test_random_small_patterns(ctx, seed):
     m = ctx.load_csr(beg, end, col)
     mss = [4, 8, 128, 200, 256][seed % 5]
     res = ctx.factor(m, max_supernode_size=mss, l_row_stats=True, pattern=True,
-                     threads_per_source=[128, 256, 512, 1024][seed % 4])
+                     threads_per_source=[128, 256, 512, 1024][seed % 4], **MODES[(seed // 3) % 4])
     r, rt = oracle_full(beg, end, col, pattern=True)
     check_full(res, r, rt, mss=mss)
     up, uc = res.pattern_u()
@@ -118,8 +134,10 @@ def test_launch_shapes_agree(ctx):
     n, rp, col = gen.random_banded(3000, bw=6, extra=2, seed=11)
     m = ctx.load_rowptr(rp, col)
     base = None
-    for tps, inflight in [(128, 0), (256, 3), (512, 1), (1024, 0), (512, 0)]:
-        res = ctx.factor(m, threads_per_source=tps, sources_in_flight=inflight, l_row_stats=True)
+    for k, (tps, inflight) in enumerate([(128, 0), (256, 3), (512, 1), (1024, 0), (512, 0),
+                                         (256, 0), (512, 2), (1024, 5)]):
+        res = ctx.factor(m, threads_per_source=tps, sources_in_flight=inflight, l_row_stats=True,
+                         **MODES[k % 4])
         got = (res.row_counts(l_rows=True), res.digests(l_rows=True), res.supernodes()[0],
                res.counts["fill_count"])
         if base is None:
@@ -195,7 +213,12 @@ def test_grid3d_64_sampled(ctx):
     np.testing.assert_array_equal(rc["nz_row_u"][rows], rr["nzU_ref"])
     np.testing.assert_array_equal(dg["dig_u_row"][rows], rr["digU"])
     # symmetric pattern: L column m has the same ids as U row m
-    np.testing.assert_array_equal(rc["nnz_l_col"], rc["nnz_u_row"])
+    bad = np.nonzero(rc["nnz_l_col"] != rc["nnz_u_row"])[0].astype(np.int32)
+    if bad.size:
+        rb = O.rows(beg, end, col, rows=bad[:8])
+        pytest.fail("L column / U row counts differ at %s: L col %s, U row %s, oracle %s" % (
+            bad[:8].tolist(), rc["nnz_l_col"][bad[:8]].tolist(), rc["nnz_u_row"][bad[:8]].tolist(),
+            rb["nnzU"].tolist()))
     flags, _ = res.supernodes()
     chunks = [0, 1, 500, (n - 1) // 256]
     ref = _chunk_supernode_flags(beg, end, col, n, 256, chunks)
@@ -234,6 +257,33 @@ def test_circuit_like_sampled(ctx):
     assert c["nnz_l"] == int(rc["nnz_l_col"].sum())
     assert c["fill_count"] == c["nnz_u"] + c["nnz_l"] - (int(rp[-1]) - n)
     res.close()
+    m.close()
+
+
+@pytest.fixture(scope="module")
+def circuit_40k():
+    from gsofatpds_b200 import gen
+    n, rp, col = gen.circuit_like(n=40000, target_nnz=int(5830000 * 40000 / 659033), seed=9)
+    beg, end = gen.csr_to_beg_end(rp)
+    r = O.rows(beg, end, col)
+    tb, te, tc = O.transpose(beg, end, col)
+    rt = O.rows(tb, te, tc)
+    return rp, col, r, rt
+
+
+@pytest.mark.parametrize("tps,ring", [(128, 16), (256, 16), (512, 16), (1024, 32), (512, 4)])
+def test_closure_reuse_repeatable(ctx, circuit_40k, tps, ring):
+    """Every U row and L column of a 40k circuit-like matrix, several runs:
+    the closure ring and its merges must never depend on thread timing."""
+    rp, col, r, rt = circuit_40k
+    m = ctx.load_rowptr(rp, col)
+    for _ in range(3):
+        res = ctx.factor(m, threads_per_source=tps, cached_closures=ring, chunk_sources=64)
+        rc = res.row_counts()
+        np.testing.assert_array_equal(rc["nnz_u_row"], r["nnzU"])
+        np.testing.assert_array_equal(rc["nnz_l_col"], rt["nnzU"])
+        np.testing.assert_array_equal(res.digests()["dig_u_row"], r["digU"])
+        res.close()
     m.close()
 
 
