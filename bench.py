@@ -208,9 +208,13 @@ def main():
         dist.init_process_group("nccl", timeout=timedelta(seconds=600),
                                 device_id=torch.device("cuda", local))
 
-    from gsofatpds_b200 import Context
+    from gsofatpds_b200 import Context, replicas
 
     (n, rp, col), mss = make_workload(args.workload)
+    if world > 1:
+        chk = int(np.bitwise_xor.reduce(col.astype(np.int64) * 2654435761 + np.arange(col.size)))
+        if not replicas.same_input_on_all_ranks(chk, dist, "cuda"):
+            raise SystemExit("ranks built different inputs")
     nnz = int(rp[-1])
     ctx = Context(local)
     stream = torch.cuda.Stream()  # events and the library share this stream
@@ -251,13 +255,9 @@ def main():
         r.close()
     barrier()
     clk = clocks.stop()
-    tot_ms = float(sum(step_ms))
-    t = torch.tensor([tot_ms], dtype=torch.float64, device="cuda")
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    max_ms = float(t.item())
+    max_ms = replicas.max_over_ranks(float(sum(step_ms)), dist if world > 1 else None, "cuda")
     edges = counts["edges_alg"]
-    value = world * args.steps * edges / (max_ms / 1e3) / 1e9
+    value = replicas.job_throughput(world, args.steps, edges, max_ms) / 1e9
 
     # ---- end to end through the C-ABI with host buffers
     beg = torch.from_numpy(np.ascontiguousarray(rp[:-1])).pin_memory()
@@ -292,10 +292,8 @@ def main():
         L.gsofa_result_destroy(rh)
         L.gsofa_matrix_destroy(mh)
     barrier()
-    t = torch.tensor([float(sum(e2e_ms))], dtype=torch.float64, device="cuda")
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    e2e_value = world * args.steps * edges / (float(t.item()) / 1e3) / 1e9
+    e2e_max = replicas.max_over_ranks(float(sum(e2e_ms)), dist if world > 1 else None, "cuda")
+    e2e_value = replicas.job_throughput(world, args.steps, edges, e2e_max) / 1e9
     h2d = (2 * n + nnz) * 4
     d2h = 3 * n * 4
 

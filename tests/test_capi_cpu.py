@@ -1,0 +1,55 @@
+"""CPU-side checks of the C-ABI library: it loads, exports every function
+include/gsofa.h declares, and reports (never aborts) when there is no GPU."""
+import ctypes
+import os
+import re
+import subprocess
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def header_functions():
+    src = open(os.path.join(ROOT, "include", "gsofa.h")).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    return sorted(set(re.findall(r"\b(gsofa_[a-z_0-9]+)\s*\(", src)))
+
+
+def test_library_exports_every_declared_function():
+    from gsofatpds_b200 import _lib
+    L = _lib.load()
+    declared = header_functions()
+    assert len(declared) >= 20
+    missing = [f for f in declared if not hasattr(L, f)]
+    assert not missing, missing
+    assert sorted(_lib.EXPORTS) == declared
+
+
+def test_status_strings_and_defaults():
+    from gsofatpds_b200 import _lib
+    L = _lib.load()
+    for code in range(0, 10):
+        assert L.gsofa_status_string(code)
+    o = _lib.Opts()
+    assert L.gsofa_opts_default(ctypes.byref(o)) == 0
+    assert o.max_supernode_size == 128 and o.flags == (_lib.SUPERNODES | _lib.DIGESTS)
+
+
+def test_no_gpu_is_an_error_code_not_a_crash():
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    from gsofatpds_b200 import Context, GsofaError, _lib
+    with pytest.raises(GsofaError) as e:
+        Context(0)
+    assert e.value.status == _lib.ERR_CUDA
+    L = _lib.load()
+    argv = (ctypes.c_char_p * 3)(b"x", b"y", b"z")
+    assert L.gsofa_symbfact_min_id(3, argv, 0, None, None, None, None) == _lib.ERR_ARG
+
+
+def test_cli_usage_without_arguments():
+    from gsofatpds_b200 import _lib
+    out = subprocess.run([_lib.CLI_PATH], capture_output=True, text=True, timeout=60)
+    assert out.returncode == 1 and "usage" in out.stderr
