@@ -19,6 +19,7 @@ ERR_OVERFLOW = 5
 ERR_CUDA = 6
 ERR_UNSUPPORTED = 7
 ERR_BUSY = 8
+ERR_SCRATCH = 9
 
 SUPERNODES = 1 << 0
 L_ROW_STATS = 1 << 1
@@ -35,7 +36,7 @@ EXPORTS = [
     "gsofa_factor_symbolic", "gsofa_factor_batch", "gsofa_result_counts",
     "gsofa_result_row_counts", "gsofa_result_digests", "gsofa_result_supernodes",
     "gsofa_result_lmask", "gsofa_result_pattern_u", "gsofa_result_pattern_l",
-    "gsofa_result_destroy", "gsofa_symbfact_min_id",
+    "gsofa_result_destroy", "gsofa_symbfact_min_id", "gsofa_factor_symbolic_noalloc",
 ]
 
 
@@ -96,6 +97,7 @@ def load():
         "gsofa_result_pattern_u": [vp, vp, vp, i64],
         "gsofa_result_pattern_l": [vp, vp, vp, i64],
         "gsofa_result_destroy": [vp],
+        "gsofa_factor_symbolic_noalloc": [vp, ctypes.POINTER(Opts), vp, vp, vp, vp, vp, vp, vp],
         "gsofa_symbfact_min_id": [ctypes.c_int, ctypes.POINTER(ctypes.c_char_p), ctypes.c_int,
                                   ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(ctypes.c_double),
                                   ctypes.POINTER(i32), ctypes.POINTER(ctypes.c_uint64)],

@@ -508,6 +508,19 @@ int64_t parse_ints(const std::string& s, size_t* pos, int64_t count, int32_t* ou
 
 }  // namespace
 
+bool gsofa::matrix_view(const void* mat, MatrixView* out) {
+    const gsofa_matrix* m = static_cast<const gsofa_matrix*>(mat);
+    if (!m || !out || !m->ctx) return false;
+    out->device = m->ctx->device;
+    out->n = m->n;
+    out->rowptr = m->rowptr;
+    out->col = m->col;
+    out->trowptr = m->trowptr;
+    out->tcol = m->tcol;
+    out->wdeg = m->wdeg;
+    return true;
+}
+
 // ============================================================================
 extern "C" {
 

@@ -93,4 +93,17 @@ cudaError_t launch_pattern_ptrs(int32_t n, const int32_t* nnz_u, const int32_t* 
                                 size_t scan_tmp_bytes, cudaStream_t stream);
 size_t pattern_scan_bytes(int32_t n);
 
+// Device-resident view of a loaded matrix (gsofa_capi.cpp), for entry points
+// that live in other translation units.
+struct MatrixView {
+    int device;
+    int32_t n;
+    const int32_t* rowptr;
+    const int32_t* col;
+    const int32_t* trowptr;
+    const int32_t* tcol;
+    const int32_t* wdeg;
+};
+bool matrix_view(const void* mat, MatrixView* out);
+
 }  // namespace gsofa

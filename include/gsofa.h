@@ -33,6 +33,7 @@ extern "C" {
 #define GSOFA_ERR_CUDA 6         /* CUDA runtime error (message in last_error) */
 #define GSOFA_ERR_UNSUPPORTED 7  /* size or option outside what is built     */
 #define GSOFA_ERR_BUSY 8         /* serving queue full / ticket not finished */
+#define GSOFA_ERR_SCRATCH 9      /* problem larger than the no-allocation scratch area */
 
 typedef struct gsofa_ctx gsofa_ctx;
 typedef struct gsofa_matrix gsofa_matrix;
@@ -166,6 +167,41 @@ int gsofa_result_lmask(const gsofa_result* res, uint32_t* mask4n);
 int gsofa_result_pattern_u(const gsofa_result* res, int64_t* ptr, int32_t* cols, int64_t cap);
 int gsofa_result_pattern_l(const gsofa_result* res, int64_t* ptr, int32_t* rows, int64_t cap);
 int gsofa_result_destroy(gsofa_result* res);
+
+/* ---- factorization without device allocation --------------------------------- */
+/* No counterpart in the reference: an addition for callers that cannot call
+ * cudaMalloc at factorization time (a host framework that owns all device
+ * memory through its own pool, or a loop that must not allocate after its
+ * set-up).  The matrix is loaded beforehand with gsofa_load_csr; the results
+ * go to caller-owned device buffers; the kernel's scratch (work counter,
+ * status, descriptor, per-CTA queues and closure rings) comes from one static
+ * __device__ array of GSOFA_NOALLOC_SCRATCH_BYTES that every GPU loading this
+ * library holds until exit.  Nothing is allocated: no cudaMalloc, cudaFree or
+ * allocating library call.
+ *   - Size limit: a matrix of order n needs 4n bytes of queue plus
+ *     cached_closures * (n/8 + 24) bytes of closure ring per CTA (plus n/8
+ *     bytes of bitmap when n > ~1.8M); the grid shrinks to what fits and
+ *     GSOFA_ERR_SCRATCH is returned when not even one CTA fits (n above
+ *     roughly 12M with the default 8 cached closures).
+ *   - The first call made for a device looks up the array's device address
+ *     (cudaGetSymbolAddress) with that device current; make that first call
+ *     before any stream capture.
+ *   - Every call shares the array and leaves its contents behind; the work
+ *     counter and status word are cleared by each call.  Calls that overlap
+ *     on the GPU (other streams, other threads) race on the array.
+ *   - Outputs (device pointers, n entries each unless noted): d_nnz_u_row,
+ *     d_nz_row_u, d_nnz_l_col as in gsofa_result_row_counts; d_lmask 4n words
+ *     as gsofa_result_lmask; d_supernode_flags n bytes (needed only with
+ *     GSOFA_SUPERNODES); d_counters 8 entries: fills, edges_alg,
+ *     vertices_alg, edges_traversed, supernodes detected (printed count - 1),
+ *     nnz_u, nnz_l, unused.
+ *   - GSOFA_L_ROW_STATS and GSOFA_PATTERN are not available here; digests are
+ *     not computed.  Synchronous on cuda_stream (NULL = legacy stream). */
+#define GSOFA_NOALLOC_SCRATCH_BYTES (64u << 20)
+int gsofa_factor_symbolic_noalloc(const gsofa_matrix* mat, const gsofa_opts* opts,
+                                  void* cuda_stream, int32_t* d_nnz_u_row, int32_t* d_nz_row_u,
+                                  int32_t* d_nnz_l_col, uint32_t* d_lmask,
+                                  int8_t* d_supernode_flags, uint64_t* d_counters);
 
 /* ---- reference-shaped entry point ------------------------------------------ */
 /* Same argument layouts as the reference executables:

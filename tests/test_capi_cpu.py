@@ -45,6 +45,8 @@ def test_no_gpu_is_an_error_code_not_a_crash():
         Context(0)
     assert e.value.status == _lib.ERR_CUDA
     L = _lib.load()
+    assert L.gsofa_factor_symbolic_noalloc(None, None, None, None, None, None, None, None,
+                                           None) == _lib.ERR_ARG
     argv = (ctypes.c_char_p * 3)(b"x", b"y", b"z")
     assert L.gsofa_symbfact_min_id(3, argv, 0, None, None, None, None) == _lib.ERR_ARG
 
