@@ -37,6 +37,7 @@ EXPORTS = [
     "gsofa_result_row_counts", "gsofa_result_digests", "gsofa_result_supernodes",
     "gsofa_result_lmask", "gsofa_result_pattern_u", "gsofa_result_pattern_l",
     "gsofa_result_destroy", "gsofa_symbfact_min_id", "gsofa_factor_symbolic_noalloc",
+    "gsofa_autotune",
 ]
 
 
@@ -97,6 +98,7 @@ def load():
         "gsofa_result_pattern_u": [vp, vp, vp, i64],
         "gsofa_result_pattern_l": [vp, vp, vp, i64],
         "gsofa_result_destroy": [vp],
+        "gsofa_autotune": [vp, vp, ctypes.POINTER(Opts)],
         "gsofa_factor_symbolic_noalloc": [vp, ctypes.POINTER(Opts), vp, vp, vp, vp, vp, vp, vp],
         "gsofa_symbfact_min_id": [ctypes.c_int, ctypes.POINTER(ctypes.c_char_p), ctypes.c_int,
                                   ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(ctypes.c_double),

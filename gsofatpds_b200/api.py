@@ -102,6 +102,14 @@ class Context:
                    (0 if merge else C.NO_MERGE))
         return o
 
+    def autotune(self, mat, **kw):
+        """Fastest (threads_per_source, chunk_sources, cached_closures) for
+        `mat`, measured on the device; returns them as keyword arguments."""
+        o = self.opts(**kw)
+        self._check(self._L.gsofa_autotune(self._h, mat.handle, ctypes.byref(o)), "autotune")
+        return dict(threads_per_source=o.threads_per_source, chunk_sources=o.chunk_sources,
+                    cached_closures=o.cached_closures)
+
     def factor(self, mat, **kw):
         o = self.opts(**kw)
         h = ctypes.c_void_p()

@@ -5,6 +5,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <map>
 #include <cerrno>
 #include <chrono>
 #include <cstdarg>
@@ -35,6 +36,8 @@ struct gsofa_ctx {
     cudaEvent_t ev0 = nullptr, ev1 = nullptr, evt = nullptr;
     std::recursive_mutex mu;
     std::string err;
+    // autotuner choices per size class (log2 n, mean row length)
+    std::map<std::pair<int, int>, gsofa_opts> tuned;
     // pinned staging
     unsigned long long* h_counters = nullptr;  // CNT_SLOTS
     int32_t* h_status = nullptr;
@@ -160,8 +163,17 @@ constexpr int kDefaultBuAlpha = 0;  // top-down only unless a caller asks
 constexpr int kDefaultBuBeta = 24;
 constexpr int kBuMinSource = 2048;
 constexpr int kDefaultHeavyRow = 64;
-constexpr int kDefaultChunk = 64;
-constexpr int kDefaultRing = 16;
+constexpr int kDefaultRing = 32;
+
+// Default chunk (consecutive sources per work item): about four chunks per
+// CTA so the dynamic schedule can balance, between 16 and 512 sources.  Long
+// chunks amortise each chunk's first source, which has nothing to reuse.
+long long default_chunk(long long total_sources, int grid) {
+    long long c = total_sources / (4ll * (grid > 0 ? grid : 1));
+    long long p = 16;
+    while (p * 2 <= c && p < 512) p *= 2;
+    return p;
+}
 
 // Default CTA size: about 1024 resident threads per SM (the kernel is held
 // to 64 registers), given how many shared-memory bitmaps fit per SM.
@@ -318,17 +330,20 @@ MatDesc make_desc(const gsofa_matrix* m, const gsofa_result* r, long long base) 
 // Runs the traversal (and optionally supernodes / pattern) for `count`
 // matrices in one persistent launch.  results[i] must be freshly allocated.
 int run_factor(gsofa_ctx* ctx, const gsofa_matrix* const* mats, int32_t count,
-               const gsofa_opts* o, gsofa_result** res) {
+               const gsofa_opts* o, gsofa_result** res, long long sample_stride = 1) {
     int32_t nmax = 0;
     long long items = 0;
-    const long long chunk = o->chunk_sources > 0 ? o->chunk_sources : kDefaultChunk;
+    long long total_sources = 0;
     for (int32_t i = 0; i < count; i++) {
         nmax = std::max(nmax, mats[i]->n);
-        items += 2ll * ((mats[i]->n + chunk - 1) / chunk);
+        total_sources += 2ll * mats[i]->n;
     }
     LaunchCfg cfg;
     int rc = plan_launch(ctx, std::max(nmax, 1), o, &cfg);
     if (rc) return rc;
+    const long long chunk =
+        o->chunk_sources > 0 ? o->chunk_sources : default_chunk(total_sources, cfg.grid);
+    for (int32_t i = 0; i < count; i++) items += 2ll * ((mats[i]->n + chunk - 1) / chunk);
     rc = ensure(ctx, &ctx->queue, &ctx->queue_bytes, (size_t)cfg.grid * (size_t)std::max(nmax, 1) * 4);
     if (rc) return rc;
     if (!cfg.smem_bitmap) {
@@ -363,7 +378,8 @@ int run_factor(gsofa_ctx* ctx, const gsofa_matrix* const* mats, int32_t count,
     TraverseLaunch L{};
     L.mats = reinterpret_cast<const MatDesc*>(ddesc);
     L.nmats = count;
-    L.total_items = items;
+    L.total_items = sample_stride > 1 ? (items + sample_stride - 1) / sample_stride : items;
+    L.sample_stride = sample_stride > 1 ? sample_stride : 1;
     L.work_counter = wc;
     L.queue = reinterpret_cast<int32_t*>(ctx->queue);
     L.queue_stride = std::max(nmax, 1);
@@ -377,7 +393,7 @@ int run_factor(gsofa_ctx* ctx, const gsofa_matrix* const* mats, int32_t count,
     L.gprev = reinterpret_cast<uint32_t*>(ctx->gprev);
     L.merge = merge ? 1 : 0;
     L.ring = ring;
-    L.chunk = o->chunk_sources > 0 ? o->chunk_sources : kDefaultChunk;
+    L.chunk = (int)chunk;
     L.heavy_len = o->heavy_row > 0 ? ((o->heavy_row + 3) & ~3) : kDefaultHeavyRow;
 
     CK(cudaEventRecord(ctx->ev0, ctx->stream));
@@ -834,6 +850,116 @@ int gsofa_factor_batch(gsofa_ctx* ctx, const gsofa_matrix* const* mats, int32_t 
         return rc;
     }
     for (int32_t i = 0; i < count; i++) results[i] = res[i];
+    return GSOFA_OK;
+}
+
+// Times candidate launch shapes on an evenly spread sample of the matrix's
+// work items (large matrices) or on the whole matrix (small ones) and keeps
+// the fastest.  The candidates differ only in speed: every setting gives the
+// same results.  Choices are cached per size class in the context.
+int gsofa_autotune(gsofa_ctx* ctx, const gsofa_matrix* mat, gsofa_opts* opts) {
+    if (!ctx || !mat || !opts || mat->ctx != ctx) return GSOFA_ERR_ARG;
+    std::lock_guard<std::recursive_mutex> g(ctx->mu);
+    int rc = validate_opts(ctx, opts);
+    if (rc) return rc;
+    if (mat->n <= 0) return GSOFA_OK;
+    int lg = 0;
+    while ((1ll << (lg + 1)) <= (long long)mat->n) lg++;
+    const int deg = (int)((mat->nnz + mat->n / 2) / mat->n);
+    const std::pair<int, int> key(lg, deg);
+    auto it = ctx->tuned.find(key);
+    if (it != ctx->tuned.end()) {
+        opts->threads_per_source = it->second.threads_per_source;
+        opts->chunk_sources = it->second.chunk_sources;
+        opts->cached_closures = it->second.cached_closures;
+        return GSOFA_OK;
+    }
+    if (cudaSetDevice(ctx->device) != cudaSuccess) return set_err(ctx, GSOFA_ERR_CUDA, "cudaSetDevice");
+    gsofa_opts base = *opts;
+    base.flags &= ~(uint32_t)(GSOFA_SUPERNODES | GSOFA_PATTERN | GSOFA_L_ROW_STATS);
+    // reference timing with the defaults picks the sampling rate
+    gsofa_result* r = nullptr;
+    rc = result_alloc(ctx, mat->n, base.flags, base.max_supernode_size, &r);
+    if (rc) return rc;
+    const gsofa_matrix* const mats[1] = {mat};
+    gsofa_result* rr[1] = {r};
+    rc = run_factor(ctx, mats, 1, &base, rr);
+    if (rc) { result_free(r); return rc; }
+    const double full_ms = r->counts.ms_traverse;
+    // Full runs while they are short; above 2 s time every stride-th work
+    // item, keeping at least 16 items per CTA so the tail does not dominate.
+    long long stride = 1;
+    if (full_ms > 2000.0) {
+        LaunchCfg c0;
+        if (plan_launch(ctx, mat->n, &base, &c0) == GSOFA_OK) {
+            const long long items = 2ll * (mat->n / 16 + 1);
+            stride = (long long)(full_ms / 1000.0);
+            while (stride > 1 && items / stride < 16ll * c0.grid) stride--;
+        }
+    }
+    auto time_opts = [&](const gsofa_opts& p, double* ms) -> int {
+        LaunchCfg c;
+        if (plan_launch(ctx, mat->n, &p, &c) != GSOFA_OK) {
+            ctx->err.clear();
+            *ms = 1e300;
+            return GSOFA_OK;
+        }
+        int e = run_factor(ctx, mats, 1, &p, rr, stride);
+        *ms = e ? 1e300 : r->counts.ms_traverse;
+        return e;
+    };
+    // coordinate descent from the defaults: CTA size, closure ring, chunk
+    gsofa_opts best = base;
+    double best_ms = 0;
+    rc = time_opts(best, &best_ms);
+    if (rc) { result_free(r); return rc; }
+    {
+        LaunchCfg c0;
+        if (plan_launch(ctx, mat->n, &base, &c0) == GSOFA_OK) best.threads_per_source = c0.block;
+        ctx->err.clear();
+    }
+    const int tps_c[] = {256, 512, 1024};
+    for (int tps : tps_c) {
+        if (tps == best.threads_per_source) continue;
+        gsofa_opts p = best;
+        p.threads_per_source = tps;
+        double ms;
+        if ((rc = time_opts(p, &ms))) { result_free(r); return rc; }
+        if (ms < best_ms) { best_ms = ms; best = p; }
+    }
+    const int ring_c[] = {1, 8, 32};
+    const int ring_now = best.cached_closures > 0 ? best.cached_closures : kDefaultRing;
+    best.cached_closures = ring_now;
+    for (int ring : ring_c) {
+        if (ring == ring_now) continue;
+        gsofa_opts p = best;
+        p.cached_closures = ring;
+        double ms;
+        if ((rc = time_opts(p, &ms))) { result_free(r); return rc; }
+        if (ms < best_ms) { best_ms = ms; best = p; }
+    }
+    {
+        LaunchCfg c;
+        long long auto_chunk = 64;
+        if (plan_launch(ctx, mat->n, &best, &c) == GSOFA_OK) auto_chunk = default_chunk(2ll * mat->n, c.grid);
+        ctx->err.clear();
+        if (best.chunk_sources <= 0) best.chunk_sources = (int32_t)auto_chunk;
+        const long long cands[] = {auto_chunk / 4, auto_chunk * 2};
+        for (long long ch : cands) {
+            if (ch < 16 || ch > 1024 || ch == best.chunk_sources) continue;
+            gsofa_opts p = best;
+            p.chunk_sources = (int32_t)ch;
+            double ms;
+            if ((rc = time_opts(p, &ms))) { result_free(r); return rc; }
+            if (ms < best_ms) { best_ms = ms; best = p; }
+        }
+    }
+    (void)best_ms;
+    result_free(r);
+    ctx->tuned[key] = best;
+    opts->threads_per_source = best.threads_per_source;
+    opts->chunk_sources = best.chunk_sources;
+    opts->cached_closures = best.cached_closures;
     return GSOFA_OK;
 }
 

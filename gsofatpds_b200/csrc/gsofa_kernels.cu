@@ -83,6 +83,8 @@ struct TraverseSmem {
     int cnt[3];
     int abort_level;  // set when a cached source is reached: stop, merge, redo
     int pushed;       // ids a merge appended to the queue
+    unsigned pending; // cached sources a merge set (slots), for the next decision
+    unsigned reached[3];  // per level (rotating): cached sources first reached
 };
 
 // Bitmap words of a matrix of order n: n bits plus zero padding read by the
@@ -99,8 +101,6 @@ struct Src {
     const int32_t* __restrict__ irp;  // in-graph (bottom-up)
     const int32_t* __restrict__ icl;
     uint32_t* bm;                     // X: this source's seen bits
-    // The queue and the ring are written and read by different threads of the
-    // CTA across barriers; they are accessed at L2 (.cg) only.
     // Ring of the closures of the last `ring` sources this CTA finished in the
     // current chunk: source t lives in slot t & (ring-1).  Sources in
     // [cache_lo, src) are cached; merged_mask has the slots already merged.
@@ -110,7 +110,9 @@ struct Src {
     int32_t cache_lo;
     uint32_t merged_mask;
     int top;                          // slot of the largest merged source, -1 if none
+    uint32_t pending;                 // cached sources a merge set, not yet merged (slots)
     int* abort_flag;
+    unsigned* reached;                // slots of cached sources first reached this level
 };
 
 // The cached source held in ring slot j.
@@ -126,7 +128,7 @@ __device__ __forceinline__ bool covered(const Src& S, int top, int32_t v) {
     if (top < 0 || v > slot_source(S, top)) return false;
     // plain load: the ring is written by this kernel
     const uint32_t* y = S.ring_base + (long long)top * S.words;
-    return (__ldcg(y + (v >> 5)) >> (v & 31)) & 1u;
+    return (y[v >> 5] >> (v & 31)) & 1u;
 }
 
 // Slot of the largest source in a merged mask, or -1.
@@ -153,8 +155,10 @@ __device__ __forceinline__ bool td_edge(const Src& S, int v, int w, uint32_t& ra
         }
         return false;
     }
-    if (fresh && w >= S.cache_lo && !((S.merged_mask >> (w & (S.ring - 1))) & 1u))
+    if (fresh && w >= S.cache_lo && !((S.merged_mask >> (w & (S.ring - 1))) & 1u)) {
+        atomicOr(S.reached, 1u << (w & (S.ring - 1)));
         *(volatile int*)S.abort_flag = 1;
+    }
     return fresh;
 }
 
@@ -178,7 +182,7 @@ __device__ __forceinline__ void push4(int32_t* q, long long qcap, long long le, 
 #pragma unroll
     for (int c = 0; c < 4; c++) {
         if (f & (1u << c)) {
-            if (at < qcap) __stcg(q + at, ws[c]);
+            if (at < qcap) q[at] = ws[c];
             else atomicOr(status, DEV_ERR_QUEUE);
             at++;
         }
@@ -213,7 +217,7 @@ __device__ __forceinline__ void td_level(const Src& S, int32_t* q, long long qca
         const long long i = base + lane;
         int v = S.src, s0 = 0, plen = 0;
         if (i < le) {
-            v = __ldcg(q + i);
+            v = q[i];
             bool skip = false;
             if (S.merged_mask) skip = v == S.src || covered(S, S.top, v);
             if (!skip) {
@@ -298,8 +302,9 @@ __device__ __forceinline__ void bu_sweep(const Src& S, bool upper, int32_t* q, l
             base = __shfl_sync(FULL_MASK, base, leader);
             if (found) {
                 const long long at = le + base + __popc(bal & ((1u << lane) - 1u));
-                if (at < qcap) __stcg(q + at, (int32_t)u);
+                if (at < qcap) q[at] = (int32_t)u;
                 else atomicOr(status, DEV_ERR_QUEUE);
+                if (u >= S.cache_lo) atomicOr(S.reached, 1u << ((int)u & (S.ring - 1)));
             }
         }
     }
@@ -313,52 +318,75 @@ __device__ __forceinline__ void bu_sweep(const Src& S, bool upper, int32_t* q, l
 // appended to the queue at `at` (*pushed gets their number).  Block-wide,
 // uniform; returns the new merged mask.
 template <int BLOCK>
-__device__ __forceinline__ uint32_t merge_reached(const Src& S, uint32_t* bm, int32_t* q,
-                                                  long long at, long long qcap, int* pushed,
+__device__ __forceinline__ uint32_t merge_reached(const Src& S, uint32_t reached, uint32_t* bm,
+                                                  int32_t* q, long long at, long long qcap,
+                                                  int* pushed, uint32_t* pending_out,
                                                   int32_t* status, bool& did_merge) {
+    // The decision uses only values every thread holds identically: the
+    // level's reached mask (stable until two levels later), the pending mask
+    // and the ring, never the live bitmap.
     uint32_t add = 0;
     did_merge = false;
     uint32_t mm = S.merged_mask;
+    const uint32_t cand = (reached | S.pending) & ~mm;
+    if (!cand) return mm;
     for (int32_t t = S.src - 1; t >= S.cache_lo; t--) {
         const int slot = t & (S.ring - 1);
-        if ((mm >> slot) & 1u) continue;
-        if (!((ld_vol(bm + (t >> 5)) >> (t & 31)) & 1u)) continue;
+        if (!((cand >> slot) & 1u)) continue;
         const bool inside = covered(S, top_slot(S, mm), t);
         mm |= 1u << slot;
         if (!inside) add |= 1u << slot;
     }
-    // window [cache_lo, src) spans at most 32 ids: two words before the merge
-    const long long w0 = S.cache_lo >> 5, w1 = (S.src - 1) >> 5;
-    const uint32_t b0 = ld_vol(bm + w0), b1 = ld_vol(bm + w1);
-    // Every thread must finish reading the bitmap before any thread goes on:
-    // without this barrier a fast thread that found nothing to merge starts
-    // the next level and sets bits a slow thread is still reading, the slow
-    // thread then decides differently and the block's barriers fall out of
-    // step.
-    __syncthreads();
     if (!add) return mm;
     did_merge = true;
+    // ids in (t, src) of an added t's closure were never expanded; with only
+    // src-1 added that window is empty and the merge is a plain OR
+    int32_t lo = S.src;
+    for (uint32_t a = add; a; a &= a - 1) {
+        const int32_t t = slot_source(S, __ffs(a) - 1);
+        if (t + 1 < lo) lo = t + 1;
+    }
+    const bool window = lo < S.src;
+    // the window [lo, src) spans at most 32 ids: two words before the merge
+    const long long w0 = lo >> 5, w1 = (S.src - 1) >> 5;
+    uint32_t b0 = 0, b1 = 0;
+    if (window) {
+        b0 = ld_vol(bm + w0);
+        b1 = ld_vol(bm + w1);
+        __syncthreads();
+    }
     for (long long i = threadIdx.x; i < S.words; i += BLOCK) {
         uint32_t x = bm[i];
         for (uint32_t a = add; a; a &= a - 1)
-            x |= __ldcg(S.ring_base + (long long)(__ffs(a) - 1) * S.words + i);
+            x |= S.ring_base[(long long)(__ffs(a) - 1) * S.words + i];
         bm[i] = x;
+    }
+    if (!window) {
+        if (threadIdx.x == 0) {
+            *pushed = 0;
+            *pending_out = 0u;
+        }
+        return mm;  // the caller's barrier completes the merge
     }
     __syncthreads();
     if (threadIdx.x == 0) {
         int np = 0;
+        uint32_t pend = 0;
         const int top = top_slot(S, mm);
-        for (int32_t v = S.cache_lo; v < S.src; v++) {
+        for (int32_t v = lo; v < S.src; v++) {
             const long long w = v >> 5;
             const uint32_t before = w == w0 ? b0 : b1;
             const uint32_t bit = 1u << (v & 31);
             if ((before & bit) || !(ld_vol(bm + w) & bit)) continue;  // not set by the merge
+            // a cached source set by the merge is reached too: merge it next time
+            if (!((mm >> (v & (S.ring - 1))) & 1u)) pend |= 1u << (v & (S.ring - 1));
             if (covered(S, top, v)) continue;
-            if (at + np < qcap) __stcg(q + at + np, v);
+            if (at + np < qcap) q[at + np] = v;
             else atomicOr(status, DEV_ERR_QUEUE);
             np++;
         }
         *pushed = np;
+        *pending_out = pend;
     }
     return mm;
 }
@@ -385,8 +413,8 @@ __global__ void __launch_bounds__(BLOCK, 1024 / BLOCK) traverse_kernel(TraverseL
     for (;;) {
         if (threadIdx.x == 0) SM.item = (long long)atomicAdd(P.work_counter, 1ull);
         __syncthreads();
-        const long long item = SM.item;
-        if (item >= P.total_items) break;
+        if (SM.item >= P.total_items) break;
+        const long long item = SM.item * (P.sample_stride > 1 ? P.sample_stride : 1);
         const int mi = find_matrix(P.mats, P.nmats, item);
         const MatDesc& M = P.mats[mi];
         const int32_t n = M.n;
@@ -420,10 +448,13 @@ __global__ void __launch_bounds__(BLOCK, 1024 / BLOCK) traverse_kernel(TraverseL
             S.cache_lo = P.merge ? max(s_first, src - P.ring) : src;
             S.merged_mask = 0u;
             S.top = -1;
+            S.pending = 0u;
+            S.reached = &SM.reached[0];
             if (threadIdx.x == 0) {
                 bm[src >> 5] |= 1u << (src & 31);
-                __stcg(q, src);
+                q[0] = src;
                 SM.cnt[0] = 0;
+                SM.reached[0] = 0u;
                 SM.abort_level = 0;
             }
             __syncthreads();
@@ -441,7 +472,11 @@ __global__ void __launch_bounds__(BLOCK, 1024 / BLOCK) traverse_kernel(TraverseL
                         bottom_up = used_bu = true;
                         continue;
                     }
-                    if (threadIdx.x == 0) SM.cnt[(level + 1) % 3] = 0;
+                    if (threadIdx.x == 0) {
+                        SM.cnt[(level + 1) % 3] = 0;
+                        SM.reached[(level + 1) % 3] = 0u;
+                    }
+                    S.reached = &SM.reached[level % 3];
                     td_level<BLOCK>(S, q, qcap, lb, le, &SM.cnt[level % 3], P.status, P.heavy_len,
                                     raw, orig, trav);
                     __syncthreads();
@@ -449,16 +484,19 @@ __global__ void __launch_bounds__(BLOCK, 1024 / BLOCK) traverse_kernel(TraverseL
                     level++;
                     // a reached cached source's closure is ours: merge it
                     bool did = false;
+                    const uint32_t reached = SM.reached[(level - 1) % 3];
                     const uint32_t mm =
-                        S.cache_lo < src ? merge_reached<BLOCK>(S, bm, q, le + nxt, qcap, &SM.pushed,
-                                                                P.status, did)
-                                         : S.merged_mask;
+                        S.cache_lo < src
+                            ? merge_reached<BLOCK>(S, reached, bm, q, le + nxt, qcap, &SM.pushed,
+                                                   &SM.pending, P.status, did)
+                            : S.merged_mask;
                     if (mm != S.merged_mask) {
                         S.merged_mask = mm;
                         S.top = top_slot(S, mm);
                         if (threadIdx.x == 0) SM.abort_level = 0;
                         __syncthreads();
                         const int np = did ? SM.pushed : 0;
+                        S.pending = did ? (SM.pending & ~mm) : (S.pending & ~mm);
                         le = le + nxt + np;  // redo this level (it may have been cut short)
                     } else {
                         lb = le;
@@ -467,7 +505,11 @@ __global__ void __launch_bounds__(BLOCK, 1024 / BLOCK) traverse_kernel(TraverseL
                     if (le > qcap) le = qcap;  // unreachable: each vertex is queued once
                 } else {
                     const long long unseen = (long long)src - (le - 1);
-                    if (threadIdx.x == 0) SM.cnt[(level + 1) % 3] = 0;
+                    if (threadIdx.x == 0) {
+                        SM.cnt[(level + 1) % 3] = 0;
+                        SM.reached[(level + 1) % 3] = 0u;
+                    }
+                    S.reached = &SM.reached[level % 3];
                     bu_sweep<BLOCK>(S, false, q, qcap, le, &SM.cnt[level % 3], P.status, trav);
                     __syncthreads();
                     const int found = SM.cnt[level % 3];
@@ -476,15 +518,18 @@ __global__ void __launch_bounds__(BLOCK, 1024 / BLOCK) traverse_kernel(TraverseL
                     le = le + found;
                     if (le > qcap) le = qcap;
                     bool did = false;
+                    const uint32_t reached = SM.reached[(level - 1) % 3];
                     const uint32_t mm =
-                        S.cache_lo < src ? merge_reached<BLOCK>(S, bm, q, le, qcap, &SM.pushed,
-                                                                P.status, did)
-                                         : S.merged_mask;
+                        S.cache_lo < src
+                            ? merge_reached<BLOCK>(S, reached, bm, q, le, qcap, &SM.pushed,
+                                                   &SM.pending, P.status, did)
+                            : S.merged_mask;
                     if (mm != S.merged_mask) {
                         S.merged_mask = mm;
                         S.top = top_slot(S, mm);
                         if (threadIdx.x == 0) SM.abort_level = 0;
                         __syncthreads();
+                        S.pending = did ? (SM.pending & ~mm) : (S.pending & ~mm);
                         le = le + (did ? SM.pushed : 0);  // merged-in ids become queue entries
                         continue;  // sweep again with the merged closure
                     }
@@ -545,7 +590,7 @@ __global__ void __launch_bounds__(BLOCK, 1024 / BLOCK) traverse_kernel(TraverseL
             for (long long w = threadIdx.x; w < words; w += BLOCK) {
                 const uint32_t x = bm[w];
                 bm[w] = 0u;
-                if (keep) __stcg(keep_slot + w, x);
+                if (keep) keep_slot[w] = x;
                 if (!x || w >= nwords) continue;
                 const long long base = w << 5;
                 uint32_t lo_m, hi_m;

@@ -119,6 +119,14 @@ int gsofa_matrix_destroy(gsofa_matrix* mat);
 /* Synchronous: returns when the result is complete on the device. */
 int gsofa_factor_symbolic(gsofa_ctx* ctx, const gsofa_matrix* mat, const gsofa_opts* opts,
                           gsofa_result** out);
+/* Autotuner: times candidate launch shapes (threads_per_source,
+ * chunk_sources, cached_closures) for this matrix on a sample of its work
+ * and writes the fastest into *opts (other fields are left as given).
+ * Results never depend on these settings.  Choices are cached in the
+ * context per size class (log2 n, mean row length), so later calls for
+ * similar matrices return at once.  Replaces the reference's fixed sizing
+ * (Compute_Src_group, :1031-1048; SPO :1101-1119, :1465-1507). */
+int gsofa_autotune(gsofa_ctx* ctx, const gsofa_matrix* mat, gsofa_opts* opts);
 /* Many matrices of uneven size in one persistent launch; results[i] is the
  * result of mats[i] (identical to factoring it alone). */
 int gsofa_factor_batch(gsofa_ctx* ctx, const gsofa_matrix* const* mats, int32_t count,

@@ -287,6 +287,25 @@ def test_closure_reuse_repeatable(ctx, circuit_40k, tps, ring):
     m.close()
 
 
+def test_autotune_picks_valid_shapes_with_same_results(ctx):
+    from gsofatpds_b200 import gen
+    n, rp, col = gen.random_banded(6000, bw=5, extra=2, seed=5)
+    m = ctx.load_rowptr(rp, col)
+    tuned = ctx.autotune(m)
+    assert tuned["threads_per_source"] in (128, 256, 512, 1024)
+    assert tuned["chunk_sources"] > 0 and tuned["cached_closures"] in (1, 2, 4, 8, 16, 32)
+    assert ctx.autotune(m) == tuned  # cached for the size class
+    a = ctx.factor(m, l_row_stats=True)
+    b = ctx.factor(m, l_row_stats=True, **tuned)
+    for x, y in zip(a.row_counts(True).values(), b.row_counts(True).values()):
+        np.testing.assert_array_equal(x, y)
+    np.testing.assert_array_equal(a.supernodes()[0], b.supernodes()[0])
+    assert a.counts["fill_count"] == b.counts["fill_count"]
+    a.close()
+    b.close()
+    m.close()
+
+
 def test_batch_equals_alone(ctx):
     from gsofatpds_b200 import gen
     mats_np = [gen.grid_nd((40, 37), "5"), gen.random_banded(2500, bw=5, extra=1, seed=2),
