@@ -34,6 +34,8 @@ WORKLOADS = {
     "random_extra": "n=20000 diagonal+tridiagonal+3 uniform columns/row, mss 128",
     "grid3d_64": "64^3 7-point grid, nested-dissection order, mss 256",
     "circuit_like_100k": "circuit-like n=100000 ~0.89M nnz (profiling size), mss 128",
+    "batch512": "512 matrices, n log-uniform [2000, 60000]: 2D 5-point ND grids and random-banded "
+                "unsymmetric (bandwidth 4-32, 1-4 uniform off-band entries/row), mss 128",
 }
 
 
@@ -180,6 +182,59 @@ def run_reference(args, rank, world):
     print(json.dumps(line), flush=True)
 
 
+def run_batch(args, local):
+    """Batched form: the same 512 matrices factored back to back (one call
+    each) and as one graph-captured persistent launch."""
+    import torch
+    from gsofatpds_b200 import Context, gen
+    torch.cuda.set_device(local)
+    mats_np = gen.batch_mix(512)
+    ctx = Context(local)
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
+    ctx.set_stream(stream.cuda_stream)
+    mats = [ctx.load_rowptr(rp, col) for (_, rp, col) in mats_np]
+    kw = dict(max_supernode_size=128)
+    if not args.no_tune:
+        big = max(range(len(mats)), key=lambda i: mats[i].nnz)
+        kw.update(ctx.autotune(mats[big], **kw))
+    batch = ctx.batch(mats, **kw)
+
+    def timed(fn):
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1)
+
+    def plain():
+        for m in mats:
+            ctx.factor(m, **kw).close()
+
+    for _ in range(args.warmup):
+        plain()
+        batch.run()
+    plain_ms = [timed(plain) for _ in range(args.steps)]
+    batch_ms = [timed(batch.run) for _ in range(args.steps)]
+    edges = sum(batch.result(i).counts["edges_alg"] for i in range(len(mats)))
+    pm, bm = float(np.median(plain_ms)), float(np.median(batch_ms))
+    line = {"metric": "matrices_per_s", "value": len(mats) / (bm / 1e3), "unit": "matrices/s",
+            "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": bm,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int32",
+            "data": "synthetic", "config": {"workload": WORKLOADS["batch512"],
+                                            "launch": {k: v for k, v in kw.items()}},
+            "plain_ms_per_batch": pm, "plain_matrices_per_s": len(mats) / (pm / 1e3),
+            "speedup_vs_plain": pm / bm, "edges_alg": edges, "gteps": edges / (bm / 1e3) / 1e9,
+            "gpu_launches": 1}
+    print(json.dumps(line), flush=True)
+    batch.close()
+    for m in mats:
+        m.close()
+    ctx.close()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -198,6 +253,9 @@ def main():
 
     if args.impl == "reference":
         run_reference(args, rank, world)
+        return
+    if args.workload == "batch512":
+        run_batch(args, local)
         return
 
     import torch

@@ -37,7 +37,8 @@ EXPORTS = [
     "gsofa_result_row_counts", "gsofa_result_digests", "gsofa_result_supernodes",
     "gsofa_result_lmask", "gsofa_result_pattern_u", "gsofa_result_pattern_l",
     "gsofa_result_destroy", "gsofa_symbfact_min_id", "gsofa_factor_symbolic_noalloc",
-    "gsofa_autotune",
+    "gsofa_autotune", "gsofa_batch_create", "gsofa_batch_run", "gsofa_batch_result",
+    "gsofa_batch_destroy",
 ]
 
 
@@ -99,6 +100,10 @@ def load():
         "gsofa_result_pattern_l": [vp, vp, vp, i64],
         "gsofa_result_destroy": [vp],
         "gsofa_autotune": [vp, vp, ctypes.POINTER(Opts)],
+        "gsofa_batch_create": [vp, ctypes.POINTER(vp), i32, ctypes.POINTER(Opts), ctypes.POINTER(vp)],
+        "gsofa_batch_run": [vp],
+        "gsofa_batch_result": [vp, i32, ctypes.POINTER(vp)],
+        "gsofa_batch_destroy": [vp],
         "gsofa_factor_symbolic_noalloc": [vp, ctypes.POINTER(Opts), vp, vp, vp, vp, vp, vp, vp],
         "gsofa_symbfact_min_id": [ctypes.c_int, ctypes.POINTER(ctypes.c_char_p), ctypes.c_int,
                                   ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(ctypes.c_double),

@@ -15,7 +15,7 @@ import numpy as np
 
 from . import _lib as C
 
-__all__ = ["GsofaError", "Context", "Matrix", "Result", "symbfact_min_id"]
+__all__ = ["GsofaError", "Context", "Matrix", "Result", "Batch", "symbfact_min_id"]
 
 
 class GsofaError(RuntimeError):
@@ -117,6 +117,10 @@ class Context:
                                                   ctypes.byref(h)), "factor_symbolic")
         return Result(self, h)
 
+    def batch(self, mats, **kw):
+        """Prepared graph-captured batch (see Batch)."""
+        return Batch(self, mats, **kw)
+
     def factor_batch(self, mats, **kw):
         o = self.opts(**kw)
         k = len(mats)
@@ -136,6 +140,36 @@ class Context:
 
     def __exit__(self, *a):
         self.close()
+
+
+class Batch:
+    """Many matrices in one persistent launch captured in a CUDA graph;
+    run() replays it.  Results are owned by the batch."""
+
+    def __init__(self, ctx, mats, **kw):
+        self.ctx = ctx
+        self.mats = list(mats)  # keep the matrices alive while the batch lives
+        o = ctx.opts(**kw)
+        k = len(self.mats)
+        arr = (ctypes.c_void_p * max(k, 1))(*[m.handle for m in self.mats])
+        h = ctypes.c_void_p()
+        ctx._check(ctx._L.gsofa_batch_create(ctx.handle, arr, k, ctypes.byref(o), ctypes.byref(h)),
+                   "batch_create")
+        self._h = h
+
+    def run(self):
+        self.ctx._check(self.ctx._L.gsofa_batch_run(self._h), "batch_run")
+        return self
+
+    def result(self, i):
+        h = ctypes.c_void_p()
+        self.ctx._check(self.ctx._L.gsofa_batch_result(self._h, int(i), ctypes.byref(h)), "batch_result")
+        return Result(self.ctx, h, owned=False)
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self.ctx._L.gsofa_batch_destroy(self._h)
+            self._h = None
 
 
 class Matrix:
@@ -159,9 +193,10 @@ class Matrix:
 
 
 class Result:
-    def __init__(self, ctx, h):
+    def __init__(self, ctx, h, owned=True):
         self.ctx = ctx
         self._h = h
+        self._owned = owned
         c = C.Counts()
         ctx._check(ctx._L.gsofa_result_counts(h, ctypes.byref(c)), "result_counts")
         self.counts = {f: getattr(c, f) for f, _ in C.Counts._fields_ if f != "reserved"}
@@ -221,7 +256,8 @@ class Result:
 
     def close(self):
         if getattr(self, "_h", None):
-            self.ctx._L.gsofa_result_destroy(self._h)
+            if self._owned:
+                self.ctx._L.gsofa_result_destroy(self._h)
             self._h = None
 
 

@@ -90,6 +90,22 @@ struct gsofa_result {
     int64_t* lptr = nullptr;
     int32_t* lrows = nullptr;
     gsofa_counts counts{};
+    bool batch_owned = false;  // lives inside a gsofa_batch: not destroyed alone
+};
+
+struct gsofa_batch {
+    gsofa_ctx* ctx = nullptr;
+    int32_t count = 0;
+    gsofa_opts opts{};
+    std::vector<gsofa_result*> res;
+    void* ws = nullptr;  // private workspace (graph holds raw pointers into it)
+    size_t ws_bytes = 0;
+    unsigned long long* h_counters = nullptr;  // pinned, count * CNT_SLOTS
+    int32_t* h_status = nullptr;               // pinned
+    cudaEvent_t e0 = nullptr, et = nullptr, e1 = nullptr;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    long long items = 0;
 };
 
 // ---------------------------------------------------------------------------
@@ -316,6 +332,7 @@ MatDesc make_desc(const gsofa_matrix* m, const gsofa_result* r, long long base) 
     d.nnz_lc = r->nnz_lc;
     d.dig_lc = r->dig_lc;
     d.lmask = r->lmask;
+    d.sflags = r->sflags;
     d.nnz_lr = r->nnz_lr;
     d.dig_lr = r->dig_lr;
     d.counters = r->counters;
@@ -969,6 +986,217 @@ int gsofa_factor_symbolic(gsofa_ctx* ctx, const gsofa_matrix* mat, const gsofa_o
     return gsofa_factor_batch(ctx, &mat, 1, opts, out);
 }
 
+static void batch_free(gsofa_batch* b) {
+    if (!b) return;
+    gsofa_ctx* ctx = b->ctx;
+    if (ctx) {
+        std::lock_guard<std::recursive_mutex> g(ctx->mu);
+        cudaSetDevice(ctx->device);
+        if (b->exec) cudaGraphExecDestroy(b->exec);
+        if (b->graph) cudaGraphDestroy(b->graph);
+        for (gsofa_result* r : b->res) {
+            if (!r) continue;
+            r->batch_owned = false;
+            result_free(r);
+        }
+        dev_free(ctx, b->ws, b->ws_bytes);
+        cudaStreamSynchronize(ctx->stream);
+        if (b->h_counters) cudaFreeHost(b->h_counters);
+        if (b->h_status) cudaFreeHost(b->h_status);
+        if (b->e0) cudaEventDestroy(b->e0);
+        if (b->et) cudaEventDestroy(b->et);
+        if (b->e1) cudaEventDestroy(b->e1);
+    }
+    delete b;
+}
+
+int gsofa_batch_create(gsofa_ctx* ctx, const gsofa_matrix* const* mats, int32_t count,
+                       const gsofa_opts* opts, gsofa_batch** out) {
+    if (!ctx || !out || count <= 0 || !mats) return GSOFA_ERR_ARG;
+    *out = nullptr;
+    std::lock_guard<std::recursive_mutex> g(ctx->mu);
+    gsofa_opts o;
+    if (opts) o = *opts; else gsofa_opts_default(&o);
+    int rc = validate_opts(ctx, &o);
+    if (rc) return rc;
+    if (o.flags & GSOFA_PATTERN)
+        return set_err(ctx, GSOFA_ERR_UNSUPPORTED, "a captured batch cannot materialise patterns");
+    int32_t nmax = 1;
+    long long total_sources = 0;
+    for (int32_t i = 0; i < count; i++) {
+        if (!mats[i] || mats[i]->ctx != ctx)
+            return set_err(ctx, GSOFA_ERR_ARG, "matrix %d is null or from another context", i);
+        nmax = std::max(nmax, mats[i]->n);
+        total_sources += 2ll * mats[i]->n;
+    }
+    if (cudaSetDevice(ctx->device) != cudaSuccess) return set_err(ctx, GSOFA_ERR_CUDA, "cudaSetDevice");
+    gsofa_batch* b = new (std::nothrow) gsofa_batch();
+    if (!b) return set_err(ctx, GSOFA_ERR_OOM_BUDGET, "host allocation failed");
+    b->ctx = ctx;
+    b->count = count;
+    b->opts = o;
+    b->res.assign((size_t)count, nullptr);
+    auto fail = [&](int code) {
+        batch_free(b);
+        return code;
+    };
+    for (int32_t i = 0; i < count; i++) {
+        rc = result_alloc(ctx, mats[i]->n, o.flags, o.max_supernode_size, &b->res[(size_t)i]);
+        if (rc) return fail(rc);
+        b->res[(size_t)i]->batch_owned = true;
+    }
+    LaunchCfg cfg;
+    rc = plan_launch(ctx, nmax, &o, &cfg);
+    if (rc) return fail(rc);
+    const long long chunk =
+        o.chunk_sources > 0 ? o.chunk_sources : default_chunk(total_sources, cfg.grid);
+    const bool merge = !(o.flags & GSOFA_NO_MERGE);
+    int ring = o.cached_closures > 0 ? o.cached_closures : kDefaultRing;
+    if (ring > 32) ring = 32;
+    while (ring & (ring - 1)) ring &= ring - 1;
+    // descriptors, segment prefix, counters, workspace: one private block
+    std::vector<MatDesc> descs((size_t)count);
+    std::vector<long long> seg((size_t)count + 1, 0);
+    long long base = 0;
+    for (int32_t i = 0; i < count; i++) {
+        descs[(size_t)i] = make_desc(mats[i], b->res[(size_t)i], base);
+        base += 2ll * ((mats[i]->n + chunk - 1) / chunk);
+        seg[(size_t)i + 1] = seg[(size_t)i] + supernode_segment_count(mats[i]->n, o.max_supernode_size);
+    }
+    b->items = base;
+    const size_t sz_small = 256;
+    const size_t sz_desc = align256(sizeof(MatDesc) * (size_t)count);
+    const size_t sz_seg = align256(sizeof(long long) * ((size_t)count + 1));
+    const size_t sz_cnt = align256(8ull * CNT_SLOTS * (size_t)count);
+    const size_t sz_q = align256((size_t)cfg.grid * (size_t)nmax * 4);
+    const size_t sz_ring = merge ? align256((size_t)cfg.grid * (size_t)ring * (size_t)cfg.words * 4) : 0;
+    const size_t sz_gbm = cfg.smem_bitmap ? 0 : align256((size_t)cfg.grid * (size_t)cfg.words * 4);
+    b->ws_bytes = sz_small + sz_desc + sz_seg + sz_cnt + sz_q + sz_ring + sz_gbm;
+    rc = dev_alloc(ctx, b->ws_bytes, &b->ws);
+    if (rc) return fail(rc);
+    char* p = reinterpret_cast<char*>(b->ws);
+    unsigned long long* wc = reinterpret_cast<unsigned long long*>(p);
+    int32_t* dstatus = reinterpret_cast<int32_t*>(p + 64);
+    p += sz_small;
+    MatDesc* ddesc = reinterpret_cast<MatDesc*>(p);
+    p += sz_desc;
+    long long* dseg = reinterpret_cast<long long*>(p);
+    p += sz_seg;
+    unsigned long long* dcnt = reinterpret_cast<unsigned long long*>(p);
+    p += sz_cnt;
+    int32_t* dq = reinterpret_cast<int32_t*>(p);
+    p += sz_q;
+    uint32_t* dring = merge ? reinterpret_cast<uint32_t*>(p) : nullptr;
+    p += sz_ring;
+    uint32_t* dgbm = cfg.smem_bitmap ? nullptr : reinterpret_cast<uint32_t*>(p);
+    for (int32_t i = 0; i < count; i++) descs[(size_t)i].counters = dcnt + (size_t)i * CNT_SLOTS;
+    cudaError_t e;
+    if ((e = cudaMemcpyAsync(ddesc, descs.data(), sizeof(MatDesc) * (size_t)count,
+                             cudaMemcpyHostToDevice, ctx->stream)) != cudaSuccess ||
+        (e = cudaMemcpyAsync(dseg, seg.data(), sizeof(long long) * ((size_t)count + 1),
+                             cudaMemcpyHostToDevice, ctx->stream)) != cudaSuccess ||
+        (e = cudaStreamSynchronize(ctx->stream)) != cudaSuccess ||
+        (e = cudaMallocHost((void**)&b->h_counters, 8ull * CNT_SLOTS * (size_t)count)) != cudaSuccess ||
+        (e = cudaMallocHost((void**)&b->h_status, 64)) != cudaSuccess ||
+        (e = cudaEventCreate(&b->e0)) != cudaSuccess || (e = cudaEventCreate(&b->et)) != cudaSuccess ||
+        (e = cudaEventCreate(&b->e1)) != cudaSuccess)
+        return fail(cuda_fail(ctx, e, "batch set-up"));
+
+    TraverseLaunch L{};
+    L.mats = ddesc;
+    L.nmats = count;
+    L.total_items = b->items;
+    L.work_counter = wc;
+    L.queue = dq;
+    L.queue_stride = nmax;
+    L.gbitmap = dgbm;
+    L.bitmap_words = cfg.words;
+    L.status = dstatus;
+    L.pattern_pass = 0;
+    L.bu_alpha = o.bu_alpha > 0 ? o.bu_alpha : (o.bu_alpha < 0 ? 0 : kDefaultBuAlpha);
+    L.bu_beta = o.bu_beta > 0 ? o.bu_beta : kDefaultBuBeta;
+    L.bu_min_src = o.bu_min_source > 0 ? o.bu_min_source : kBuMinSource;
+    L.heavy_len = o.heavy_row > 0 ? ((o.heavy_row + 3) & ~3) : kDefaultHeavyRow;
+    L.gprev = dring;
+    L.chunk = (int)chunk;
+    L.merge = merge ? 1 : 0;
+    L.ring = ring;
+    L.sample_stride = 1;
+
+    // capture: reset -> traversal -> supernodes -> read-back
+    if ((e = cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeRelaxed)) != cudaSuccess)
+        return fail(cuda_fail(ctx, e, "cudaStreamBeginCapture"));
+    e = cudaMemsetAsync(b->ws, 0, 128, ctx->stream);
+    if (e == cudaSuccess) e = launch_batch_reset(ddesc, count, ctx->stream);
+    if (e == cudaSuccess && b->items > 0)
+        e = launch_traverse(L, cfg.block, cfg.grid, cfg.smem_bitmap, cfg.smem, ctx->stream);
+    if (e == cudaSuccess && (o.flags & GSOFA_SUPERNODES))
+        e = launch_supernodes_batch(ddesc, count, o.max_supernode_size, dseg, seg[(size_t)count],
+                                    ctx->stream);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(b->h_counters, dcnt, 8ull * CNT_SLOTS * (size_t)count,
+                            cudaMemcpyDeviceToHost, ctx->stream);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(b->h_status, dstatus, 4, cudaMemcpyDeviceToHost, ctx->stream);
+    cudaGraph_t graph = nullptr;
+    cudaError_t e2 = cudaStreamEndCapture(ctx->stream, &graph);
+    if (e != cudaSuccess || e2 != cudaSuccess) {
+        if (graph) cudaGraphDestroy(graph);
+        return fail(cuda_fail(ctx, e != cudaSuccess ? e : e2, "batch capture"));
+    }
+    b->graph = graph;
+    if ((e = cudaGraphInstantiate(&b->exec, b->graph, 0)) != cudaSuccess)
+        return fail(cuda_fail(ctx, e, "cudaGraphInstantiate"));
+    *out = b;
+    return GSOFA_OK;
+}
+
+int gsofa_batch_run(gsofa_batch* b) {
+    if (!b) return GSOFA_ERR_ARG;
+    gsofa_ctx* ctx = b->ctx;
+    std::lock_guard<std::recursive_mutex> g(ctx->mu);
+    if (cudaSetDevice(ctx->device) != cudaSuccess) return set_err(ctx, GSOFA_ERR_CUDA, "cudaSetDevice");
+    // events around the graph launch: the whole batch's device time
+    CK(cudaEventRecord(b->e0, ctx->stream));
+    CK(cudaGraphLaunch(b->exec, ctx->stream));
+    CK(cudaEventRecord(b->e1, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    *ctx->h_status = *b->h_status;
+    int rc = check_status(ctx);
+    if (rc) return rc;
+    float ms = 0.f;
+    CK(cudaEventElapsedTime(&ms, b->e0, b->e1));
+    for (int32_t i = 0; i < b->count; i++) {
+        gsofa_result* r = b->res[(size_t)i];
+        const unsigned long long* c = b->h_counters + (size_t)i * CNT_SLOTS;
+        gsofa_counts& k = r->counts;
+        k.n = r->n;
+        k.fill_count = c[CNT_FILLS];
+        k.nnz_l = c[CNT_NNZ_L];
+        k.nnz_u = c[CNT_NNZ_U];
+        k.nnz_lu = c[CNT_NNZ_L] + c[CNT_NNZ_U] + (uint64_t)r->n;
+        k.n_supernodes = (b->opts.flags & GSOFA_SUPERNODES) ? (int64_t)c[CNT_NSUP] + 1 : -1;
+        k.edges_alg = c[CNT_EDGES_ALG];
+        k.vertices_alg = c[CNT_VERTS_ALG];
+        k.edges_traversed = c[CNT_EDGES_TRAV];
+        k.ms_device = (double)ms;  // the whole batch (one graph launch)
+        k.ms_traverse = (double)ms;
+    }
+    return GSOFA_OK;
+}
+
+int gsofa_batch_result(const gsofa_batch* b, int32_t i, gsofa_result** res) {
+    if (!b || !res || i < 0 || i >= b->count) return GSOFA_ERR_ARG;
+    *res = b->res[(size_t)i];
+    return GSOFA_OK;
+}
+
+int gsofa_batch_destroy(gsofa_batch* b) {
+    if (!b) return GSOFA_ERR_ARG;
+    batch_free(b);
+    return GSOFA_OK;
+}
+
 int gsofa_result_counts(const gsofa_result* r, gsofa_counts* out) {
     if (!r || !out) return GSOFA_ERR_ARG;
     *out = r->counts;
@@ -1059,6 +1287,7 @@ int gsofa_result_pattern_l(const gsofa_result* r, int64_t* ptr, int32_t* rows, i
 
 int gsofa_result_destroy(gsofa_result* r) {
     if (!r) return GSOFA_ERR_ARG;
+    if (r->batch_owned) return set_err(r->ctx, GSOFA_ERR_ARG, "result belongs to a batch");
     result_free(r);
     return GSOFA_OK;
 }

@@ -40,6 +40,7 @@ struct MatDesc {
     int32_t* nnz_lc;            // n: |L column|
     uint64_t* dig_lc;           // n (or null)
     uint32_t* lmask;            // 4n: L(f+1+j, f) bits
+    int8_t* sflags;             // n: supernode flags (batched supernode kernel)
     int32_t* nnz_lr;            // n or null (L row scatter)
     uint64_t* dig_lr;           // n or null
     unsigned long long* counters;  // CNT_SLOTS
@@ -89,6 +90,11 @@ size_t canonicalize_scan_bytes(int32_t n);
 cudaError_t launch_supernodes(int32_t n, int32_t mss, const int32_t* nz_row_u,
                               const uint32_t* lmask, int8_t* flags,
                               unsigned long long* counters, cudaStream_t stream);
+cudaError_t launch_batch_reset(const MatDesc* mats, int nmats, cudaStream_t stream);
+cudaError_t launch_supernodes_batch(const MatDesc* mats, int nmats, int32_t mss,
+                                    const long long* seg_base, long long total_segments,
+                                    cudaStream_t stream);
+long long supernode_segment_count(int32_t n, int32_t mss);
 cudaError_t launch_pattern_ptrs(int32_t n, const int32_t* nnz_u, const int32_t* nnz_lc,
                                 int64_t* uptr, int64_t* lptr, void* scan_tmp,
                                 size_t scan_tmp_bytes, cudaStream_t stream);

@@ -105,7 +105,8 @@ struct Src {
     // current chunk: source t lives in slot t & (ring-1).  Sources in
     // [cache_lo, src) are cached; merged_mask has the slots already merged.
     const uint32_t* ring_base;
-    long long words;
+    long long words;                  // ring slot stride (the launch's widest bitmap)
+    long long mwords;                 // this matrix's bitmap words (what a merge ORs)
     int ring;
     int32_t cache_lo;
     uint32_t merged_mask;
@@ -355,7 +356,7 @@ __device__ __forceinline__ uint32_t merge_reached(const Src& S, uint32_t reached
         b1 = ld_vol(bm + w1);
         __syncthreads();
     }
-    for (long long i = threadIdx.x; i < S.words; i += BLOCK) {
+    for (long long i = threadIdx.x; i < S.mwords; i += BLOCK) {
         uint32_t x = bm[i];
         for (uint32_t a = add; a; a &= a - 1)
             x |= S.ring_base[(long long)(__ffs(a) - 1) * S.words + i];
@@ -437,6 +438,7 @@ __global__ void __launch_bounds__(BLOCK, 1024 / BLOCK) traverse_kernel(TraverseL
         S.bm = bm;
         S.ring_base = ring_base;
         S.words = P.bitmap_words;
+        S.mwords = words;
         S.ring = P.ring;
         S.abort_flag = &SM.abort_level;
         const bool digests = M.dig_u != nullptr;
@@ -910,65 +912,136 @@ cudaError_t launch_canonicalize(int32_t n, long long nnz_in, const int32_t* beg,
 // stays the first row.  Segments (runs between forced starts) hold <= 128
 // rows, so one warp handles one segment: 4 rows per lane, a warp max-scan
 // finds each row's start f, and the L-mask of column f answers L(r,f).
+// One segment (<= 128 rows between forced starts) of one matrix, one warp.
+// Returns this lane's count of supernode starts and splits.
+__device__ __forceinline__ unsigned long long supernode_segment(
+    long long sg, int32_t n, int32_t mss, const int32_t* __restrict__ nzu,
+    const uint32_t* __restrict__ lmask, int8_t* __restrict__ flags) {
+    const int lane = threadIdx.x & 31;
+    const long long segs_per_chunk = ((long long)mss + 127) / 128;
+    const long long c = sg / segs_per_chunk;
+    const long long k = sg % segs_per_chunk;
+    const long long start = c * mss + 128 * k;
+    long long stop = start + 128;
+    if (stop > (c + 1) * mss) stop = (c + 1) * mss;
+    if (stop > n) stop = n;
+    if (start >= stop) return 0;
+    unsigned long long count = 0;
+    int head[4];
+    long long last = -1;
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+        const long long r = start + 4 * lane + j;
+        head[j] = 0;
+        if (r < stop) {
+            head[j] = (r == start) || (nzu[r - 1] - nzu[r] != 1);
+            if (head[j]) last = r;
+        }
+    }
+    // exclusive max-scan of `last` over lanes
+    long long incl = last;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        long long t = __shfl_up_sync(FULL_MASK, incl, o);
+        if (lane >= o && t > incl) incl = t;
+    }
+    long long f = __shfl_up_sync(FULL_MASK, incl, 1);
+    if (lane == 0) f = -1;
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+        const long long r = start + 4 * lane + j;
+        if (r >= stop) continue;
+        int8_t fl;
+        if (head[j]) {
+            f = r;
+            fl = 1;
+            count++;
+        } else {
+            const long long bit = r - f - 1;  // 0..126
+            const uint32_t wv = lmask[4 * f + (bit >> 5)];
+            const bool in_l = (wv >> (bit & 31)) & 1u;
+            fl = in_l ? 0 : 2;
+            if (!in_l) count++;
+        }
+        if (flags) flags[r] = fl;
+    }
+    return count;
+}
+
+__device__ __forceinline__ long long supernode_segments(int32_t n, int32_t mss) {
+    return n <= 0 ? 0 : (((long long)n + mss - 1) / mss) * (((long long)mss + 127) / 128);
+}
+
 __global__ void supernode_kernel(int32_t n, int32_t mss, const int32_t* __restrict__ nzu,
                                  const uint32_t* __restrict__ lmask, int8_t* __restrict__ flags,
                                  unsigned long long* counters) {
     const long long gw = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31;
-    const long long segs_per_chunk = ((long long)mss + 127) / 128;
-    const long long nchunks = ((long long)n + mss - 1) / mss;
-    const long long nseg = nchunks * segs_per_chunk;
+    const long long nseg = supernode_segments(n, mss);
     unsigned long long count = 0;
-    for (long long sg = gw; sg < nseg; sg += ((long long)gridDim.x * blockDim.x) >> 5) {
-        const long long c = sg / segs_per_chunk;
-        const long long k = sg % segs_per_chunk;
-        const long long start = c * mss + 128 * k;
-        long long stop = start + 128;
-        if (stop > (c + 1) * mss) stop = (c + 1) * mss;
-        if (stop > n) stop = n;
-        if (start >= stop) continue;
-        int head[4];
-        long long last = -1;
-#pragma unroll
-        for (int j = 0; j < 4; j++) {
-            const long long r = start + 4 * lane + j;
-            head[j] = 0;
-            if (r < stop) {
-                head[j] = (r == start) || (nzu[r - 1] - nzu[r] != 1);
-                if (head[j]) last = r;
-            }
-        }
-        // exclusive max-scan of `last` over lanes
-        long long incl = last;
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            long long t = __shfl_up_sync(FULL_MASK, incl, o);
-            if (lane >= o && t > incl) incl = t;
-        }
-        long long f = __shfl_up_sync(FULL_MASK, incl, 1);
-        if (lane == 0) f = -1;
-#pragma unroll
-        for (int j = 0; j < 4; j++) {
-            const long long r = start + 4 * lane + j;
-            if (r >= stop) continue;
-            int8_t fl;
-            if (head[j]) {
-                f = r;
-                fl = 1;
-                count++;
-            } else {
-                const long long bit = r - f - 1;  // 0..126
-                const uint32_t wv = lmask[4 * f + (bit >> 5)];
-                const bool in_l = (wv >> (bit & 31)) & 1u;
-                fl = in_l ? 0 : 2;
-                if (!in_l) count++;
-            }
-            if (flags) flags[r] = fl;
-        }
-    }
+    for (long long sg = gw; sg < nseg; sg += ((long long)gridDim.x * blockDim.x) >> 5)
+        count += supernode_segment(sg, n, mss, nzu, lmask, flags);
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) count += __shfl_xor_sync(FULL_MASK, count, o);
     if (lane == 0 && count) atomicAdd(&counters[CNT_NSUP], count);
+}
+
+// All matrices of a batch in one launch: a global segment index is split
+// into (matrix, segment) by the per-matrix segment prefix seg_base[].
+__global__ void supernode_batch_kernel(const MatDesc* __restrict__ mats, int nmats, int32_t mss,
+                                       const long long* __restrict__ seg_base) {
+    const long long gw = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    const long long total = seg_base[nmats];
+    for (long long g = gw; g < total; g += ((long long)gridDim.x * blockDim.x) >> 5) {
+        int lo = 0, hi = nmats - 1;
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (seg_base[mid] <= g) lo = mid; else hi = mid - 1;
+        }
+        const MatDesc& M = mats[lo];
+        unsigned long long count =
+            supernode_segment(g - seg_base[lo], M.n, mss, M.nz_row_u, M.lmask, M.sflags);
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) count += __shfl_xor_sync(FULL_MASK, count, o);
+        if (lane == 0 && count) atomicAdd(&M.counters[CNT_NSUP], count);
+    }
+}
+
+// Zeroes the per-matrix counters (and the optional per-row L scatter
+// targets) of a batch before its traversal.
+__global__ void batch_reset_kernel(const MatDesc* __restrict__ mats, int nmats) {
+    for (int mi = blockIdx.x; mi < nmats; mi += gridDim.x) {
+        const MatDesc& M = mats[mi];
+        if (threadIdx.x < CNT_SLOTS) M.counters[threadIdx.x] = 0ull;
+        if (M.nnz_lr) {
+            for (long long i = threadIdx.x; i < M.n; i += blockDim.x) {
+                M.nnz_lr[i] = 0;
+                M.dig_lr[i] = 0ull;
+            }
+        }
+    }
+}
+
+cudaError_t launch_batch_reset(const MatDesc* mats, int nmats, cudaStream_t st) {
+    if (nmats <= 0) return cudaSuccess;
+    batch_reset_kernel<<<nmats < 148 * 8 ? nmats : 148 * 8, 256, 0, st>>>(mats, nmats);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_supernodes_batch(const MatDesc* mats, int nmats, int32_t mss,
+                                    const long long* seg_base, long long total_segments,
+                                    cudaStream_t st) {
+    if (nmats <= 0 || total_segments <= 0) return cudaSuccess;
+    const int threads = 256;
+    long long grid = (total_segments * 32 + threads - 1) / threads;
+    if (grid > 148 * 32) grid = 148 * 32;
+    supernode_batch_kernel<<<(int)grid, threads, 0, st>>>(mats, nmats, mss, seg_base);
+    return cudaGetLastError();
+}
+
+long long supernode_segment_count(int32_t n, int32_t mss) {
+    return n <= 0 ? 0 : (((long long)n + mss - 1) / mss) * (((long long)mss + 127) / 128);
 }
 
 cudaError_t launch_supernodes(int32_t n, int32_t mss, const int32_t* nzu, const uint32_t* lmask,

@@ -30,7 +30,9 @@ def from_coo(n, r, c):
     """Deduplicated, row-sorted, column-sorted CSR from coordinate lists."""
     r = np.asarray(r, np.int64)
     c = np.asarray(c, np.int64)
-    key = np.unique(r * n + c)
+    key = np.sort(r * n + c)
+    if key.size:
+        key = key[np.concatenate(([True], key[1:] != key[:-1]))]
     rows = (key // n).astype(np.int64)
     col = (key % n).astype(np.int32)
     cnt = np.bincount(rows, minlength=n)

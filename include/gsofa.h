@@ -38,6 +38,7 @@ extern "C" {
 typedef struct gsofa_ctx gsofa_ctx;
 typedef struct gsofa_matrix gsofa_matrix;
 typedef struct gsofa_result gsofa_result;
+typedef struct gsofa_batch gsofa_batch;
 
 /* ---- options -------------------------------------------------------------- */
 #define GSOFA_SUPERNODES (1u << 0)  /* detect supernodes (reference SOA :1790-2123) */
@@ -131,6 +132,22 @@ int gsofa_autotune(gsofa_ctx* ctx, const gsofa_matrix* mat, gsofa_opts* opts);
  * result of mats[i] (identical to factoring it alone). */
 int gsofa_factor_batch(gsofa_ctx* ctx, const gsofa_matrix* const* mats, int32_t count,
                        const gsofa_opts* opts, gsofa_result** results);
+
+/* A prepared batch: many matrices of uneven size in one persistent launch
+ * captured in a CUDA graph (reset, traversal over every matrix's work items,
+ * supernode detection of all of them, read-back of the totals), so each run
+ * is a single graph launch.  The batch owns its results (read them with
+ * gsofa_batch_result and the gsofa_result_* getters; do not destroy them) and
+ * a private workspace.  Matrices must stay alive while the batch exists.
+ * GSOFA_PATTERN is not available in a batch.  The reference factors one
+ * matrix per run (SOA :2965-3218); this has no counterpart there. */
+int gsofa_batch_create(gsofa_ctx* ctx, const gsofa_matrix* const* mats, int32_t count,
+                       const gsofa_opts* opts, gsofa_batch** out);
+/* Runs the captured graph; synchronous.  Results reflect the latest run;
+ * every run gives the same results. */
+int gsofa_batch_run(gsofa_batch* batch);
+int gsofa_batch_result(const gsofa_batch* batch, int32_t i, gsofa_result** res);
+int gsofa_batch_destroy(gsofa_batch* batch);
 
 typedef struct gsofa_counts {
     int32_t n;

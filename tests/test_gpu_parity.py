@@ -328,6 +328,37 @@ def test_batch_equals_alone(ctx):
         m.close()
 
 
+@pytest.mark.parametrize("mode", [0, 1, 3])
+def test_graph_batch_equals_alone_twice(ctx, mode):
+    """The graph-captured batch (one persistent launch for all matrices,
+    batched supernode kernel) replayed twice gives each matrix's own result."""
+    from gsofatpds_b200 import gen
+    mats_np = [gen.grid_nd((31, 29), "5"), gen.random_banded(3000, bw=6, extra=2, seed=12),
+               gen.random_extra(1500, 2, seed=8), gen.grid_nd((7, 6, 5), "7"),
+               gen.random_banded(200, bw=4, extra=1, seed=3), gen.random_extra(1, 0, seed=1)]
+    mats = [ctx.load_rowptr(rp, col) for (_, rp, col) in mats_np]
+    kw = dict(l_row_stats=True, max_supernode_size=[128, 8, 256, 64][mode], **MODES[mode])
+    alone = [ctx.factor(m, **kw) for m in mats]
+    b = ctx.batch(mats, **kw)
+    for _ in range(2):
+        b.run()
+        for i, ra in enumerate(alone):
+            rb = b.result(i)
+            for x, y in zip(ra.row_counts(True).values(), rb.row_counts(True).values()):
+                np.testing.assert_array_equal(x, y)
+            for x, y in zip(ra.digests(True).values(), rb.digests(True).values()):
+                np.testing.assert_array_equal(x, y)
+            np.testing.assert_array_equal(ra.supernodes()[0], rb.supernodes()[0])
+            np.testing.assert_array_equal(ra.lmask(), rb.lmask())
+            for k in ("fill_count", "nnz_l", "nnz_u", "edges_alg", "vertices_alg", "n_supernodes"):
+                assert ra.counts[k] == rb.counts[k], k
+    b.close()
+    for r in alone:
+        r.close()
+    for m in mats:
+        m.close()
+
+
 def test_global_bitmap_variant_matches(ctx):
     """Orders whose bitmap exceeds shared memory keep it in global memory;
     force that variant on a small case and compare."""
