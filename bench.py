@@ -36,6 +36,8 @@ WORKLOADS = {
     "circuit_like_100k": "circuit-like n=100000 ~0.89M nnz (profiling size), mss 128",
     "batch512": "512 matrices, n log-uniform [2000, 60000]: 2D 5-point ND grids and random-banded "
                 "unsymmetric (bandwidth 4-32, 1-4 uniform off-band entries/row), mss 128",
+    "serve": "Poisson request stream, n log-uniform [1000, 1000000], 5-27 nnz/row: 2D 5/9-point and "
+             "3D 7/27-point ND grids, random-banded unsymmetric (n capped), 40 GB budget, mss 128",
 }
 
 
@@ -235,6 +237,106 @@ def run_batch(args, local):
     ctx.close()
 
 
+def _pct(xs, q):
+    return float(np.percentile(np.asarray(xs, dtype=np.float64), q)) if len(xs) else None
+
+
+def run_serve(args, local):
+    """Serving form: a seeded Poisson request stream replayed in real time
+    through the request loop (host CSR in, result counts out), against the
+    same requests served one at a time by plain calls (load + factor each,
+    back to back; their queueing under the same arrivals is replayed from the
+    measured service times)."""
+    import torch
+    from gsofatpds_b200 import Context, gen
+    torch.cuda.set_device(local)
+    spec = gen.request_stream(count=args.serve_count, rate_hz=args.serve_rate, nmin=1000,
+                              nmax=1000000, seed=5, max_rb_n=args.serve_max_banded)
+    reqs = [(t, kind, sp, gen.make_request(kind, sp)) for (t, kind, sp) in spec]
+    nmax = max(r[3][0] for r in reqs)
+    kw = dict(max_supernode_size=128)
+    ctx = Context(local)
+    warm = [r for r in reqs if r[3][0] < 20000][:max(args.warmup, 1)]
+
+    def plain_one(rp, col):
+        m = ctx.load_rowptr(rp, col)
+        r = ctx.factor(m, **kw)
+        c = r.counts
+        r.close()
+        m.close()
+        return c
+
+    for r in warm:
+        plain_one(r[3][1], r[3][2])
+    service, plain_counts = [], []
+    for r in reqs:
+        t0 = time.perf_counter()
+        plain_counts.append(plain_one(r[3][1], r[3][2]))
+        service.append(time.perf_counter() - t0)
+    done, plain_lat = 0.0, []
+    for (t_arr, _, _, _), sv in zip(reqs, service):
+        done = max(done, t_arr) + sv
+        plain_lat.append(done - t_arr)
+    plain_makespan = done - reqs[0][0]
+
+    skw = dict(kw)
+    if args.threads_per_source:
+        skw["threads_per_source"] = args.threads_per_source
+    srv = ctx.server(max_n=nmax, budget_bytes=40 << 30, **skw)
+    for r in warm:
+        srv.wait(srv.submit_rowptr(r[3][1], r[3][2])).close()
+    sampler = ClockSampler(local)
+    sampler.start()
+    start = time.perf_counter()
+    tickets = []
+    for (t_arr, _, _, (_, rp, col)) in reqs:
+        d = start + t_arr - time.perf_counter()
+        if d > 0:
+            time.sleep(d)
+        tickets.append(srv.submit_rowptr(rp, col))
+    counts = []
+    for t in tickets:
+        r = srv.wait(t)
+        counts.append(r.counts)
+        r.close()
+    clk = sampler.stop()
+    info = [srv.info(t) for t in tickets]
+    st = srv.stats()
+    srv.close()
+    ctx.close()
+    lat = [(i["t_done_ms"] - i["t_submit_ms"]) / 1e3 for i in info]
+    wait_admit = [(i["t_admit_ms"] - i["t_submit_ms"]) for i in info]
+    build = [(i["t_publish_ms"] - i["t_admit_ms"]) for i in info]
+    run = [(i["t_done_ms"] - i["t_publish_ms"]) for i in info]
+    makespan = (max(i["t_done_ms"] for i in info) - min(i["t_submit_ms"] for i in info)) / 1e3
+    same = all(a["fill_count"] == b["fill_count"] and a["n_supernodes"] == b["n_supernodes"]
+               and a["edges_alg"] == b["edges_alg"] for a, b in zip(counts, plain_counts))
+    edges = sum(c["edges_alg"] for c in counts)
+    k = len(reqs)
+    h2d = sum(4 * (r[3][0] * 2 + r[3][2].shape[0]) for r in reqs)
+    line = {"metric": "matrices_per_s", "value": k / makespan, "unit": "matrices/s", "n_gpus": 1,
+            "steps": 1, "warmup": len(warm), "ms_per_step": makespan * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int32",
+            "data": "synthetic",
+            "config": {"workload": WORKLOADS["serve"], "requests": k, "rate_hz": args.serve_rate,
+                       "banded_n_cap": args.serve_max_banded, "max_n": nmax,
+                       "budget_gb": 40, "grid": st["grid"], "block": st["block"]},
+            "p50_ms": _pct(lat, 50) * 1e3, "p99_ms": _pct(lat, 99) * 1e3,
+            "plain_matrices_per_s": k / plain_makespan, "plain_p50_ms": _pct(plain_lat, 50) * 1e3,
+            "plain_p99_ms": _pct(plain_lat, 99) * 1e3, "speedup_vs_plain": plain_makespan / makespan,
+            "plain_service_s": float(sum(service)), "identical_to_plain": same,
+            "edges_alg": edges, "gteps": edges / makespan / 1e9,
+            "stage_ms": {"admit_wait_p50": _pct(wait_admit, 50), "build_p50": _pct(build, 50),
+                         "build_p99": _pct(build, 99), "run_p50": _pct(run, 50),
+                         "run_p99": _pct(run, 99)},
+            "max_in_flight": st["max_in_flight"], "kernel_launches": st["kernel_launches"],
+            "peak_bytes": st["peak_bytes"],
+            "e2e": {"value": k / makespan, "unit": "matrices/s", "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": 8 * 8 * k},
+            "clocks": clk, "gpu_launches": st["kernel_launches"]}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -245,6 +347,10 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--threads-per-source", type=int, default=0)
     ap.add_argument("--no-tune", action="store_true", help="skip the autotuner (library defaults)")
+    ap.add_argument("--serve-count", type=int, default=48)
+    ap.add_argument("--serve-rate", type=float, default=20.0, help="Poisson arrivals per second")
+    ap.add_argument("--serve-max-banded", type=int, default=100000,
+                    help="largest random-banded request (their fill grows as n^2)")
     args = ap.parse_args()
 
     rank = int(os.environ.get("RANK", "0"))
@@ -256,6 +362,9 @@ def main():
         return
     if args.workload == "batch512":
         run_batch(args, local)
+        return
+    if args.workload == "serve":
+        run_serve(args, local)
         return
 
     import torch

@@ -5,7 +5,8 @@ include/gsofa.h); this package is its Python host interface plus the seeded
 input generators.  Importing works without a GPU; the first call that needs
 the library loads it and raises if it is missing.
 """
-from .api import Batch, Context, GsofaError, Matrix, Result, symbfact_min_id  # noqa: F401
+from .api import Batch, Context, GsofaError, Matrix, Result, Server, symbfact_min_id  # noqa: F401
 from . import gen  # noqa: F401
 
-__all__ = ["Batch", "Context", "GsofaError", "Matrix", "Result", "symbfact_min_id", "gen"]
+__all__ = ["Batch", "Context", "GsofaError", "Matrix", "Result", "Server", "symbfact_min_id",
+           "gen"]

@@ -38,7 +38,9 @@ EXPORTS = [
     "gsofa_result_lmask", "gsofa_result_pattern_u", "gsofa_result_pattern_l",
     "gsofa_result_destroy", "gsofa_symbfact_min_id", "gsofa_factor_symbolic_noalloc",
     "gsofa_autotune", "gsofa_batch_create", "gsofa_batch_run", "gsofa_batch_result",
-    "gsofa_batch_destroy",
+    "gsofa_batch_destroy", "gsofa_server_create", "gsofa_server_submit", "gsofa_server_poll",
+    "gsofa_server_wait", "gsofa_server_ticket_info", "gsofa_server_get_stats",
+    "gsofa_server_destroy", "gsofa_server_last_error",
 ]
 
 
@@ -63,6 +65,22 @@ class Counts(ctypes.Structure):
                 ("n_supernodes", ctypes.c_int64), ("edges_alg", ctypes.c_uint64),
                 ("vertices_alg", ctypes.c_uint64), ("edges_traversed", ctypes.c_uint64),
                 ("ms_device", ctypes.c_double), ("ms_traverse", ctypes.c_double)]
+
+
+class TicketInfo(ctypes.Structure):
+    _fields_ = [("t_submit_ms", ctypes.c_double), ("t_admit_ms", ctypes.c_double),
+                ("t_publish_ms", ctypes.c_double), ("t_done_ms", ctypes.c_double),
+                ("footprint_bytes", ctypes.c_uint64), ("status", ctypes.c_int32),
+                ("n", ctypes.c_int32)]
+
+
+class ServerStats(ctypes.Structure):
+    _fields_ = [("submitted", ctypes.c_uint64), ("completed", ctypes.c_uint64),
+                ("failed", ctypes.c_uint64), ("kernel_launches", ctypes.c_uint64),
+                ("items_published", ctypes.c_uint64), ("bytes_in_use", ctypes.c_uint64),
+                ("peak_bytes", ctypes.c_uint64), ("fixed_bytes", ctypes.c_uint64),
+                ("grid", ctypes.c_int32), ("block", ctypes.c_int32),
+                ("max_in_flight", ctypes.c_int32), ("reserved", ctypes.c_int32)]
 
 
 _lib = None
@@ -105,6 +123,13 @@ def load():
         "gsofa_batch_result": [vp, i32, ctypes.POINTER(vp)],
         "gsofa_batch_destroy": [vp],
         "gsofa_factor_symbolic_noalloc": [vp, ctypes.POINTER(Opts), vp, vp, vp, vp, vp, vp, vp],
+        "gsofa_server_create": [vp, ctypes.POINTER(Opts), i32, ctypes.c_size_t, ctypes.POINTER(vp)],
+        "gsofa_server_submit": [vp, i32, i64, vp, vp, vp, ctypes.POINTER(ctypes.c_uint64)],
+        "gsofa_server_poll": [vp, ctypes.c_uint64, ctypes.POINTER(vp)],
+        "gsofa_server_wait": [vp, ctypes.c_uint64, ctypes.c_double, ctypes.POINTER(vp)],
+        "gsofa_server_ticket_info": [vp, ctypes.c_uint64, ctypes.POINTER(TicketInfo)],
+        "gsofa_server_get_stats": [vp, ctypes.POINTER(ServerStats)],
+        "gsofa_server_destroy": [vp],
         "gsofa_symbfact_min_id": [ctypes.c_int, ctypes.POINTER(ctypes.c_char_p), ctypes.c_int,
                                   ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(ctypes.c_double),
                                   ctypes.POINTER(i32), ctypes.POINTER(ctypes.c_uint64)],
@@ -115,6 +140,8 @@ def load():
         f.restype = ctypes.c_int
     L.gsofa_last_error.argtypes = [vp]
     L.gsofa_last_error.restype = ctypes.c_char_p
+    L.gsofa_server_last_error.argtypes = [vp]
+    L.gsofa_server_last_error.restype = ctypes.c_char_p
     L.gsofa_status_string.argtypes = [ctypes.c_int]
     L.gsofa_status_string.restype = ctypes.c_char_p
     _ = u32

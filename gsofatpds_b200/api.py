@@ -15,7 +15,7 @@ import numpy as np
 
 from . import _lib as C
 
-__all__ = ["GsofaError", "Context", "Matrix", "Result", "Batch", "symbfact_min_id"]
+__all__ = ["GsofaError", "Context", "Matrix", "Result", "Batch", "Server", "symbfact_min_id"]
 
 
 class GsofaError(RuntimeError):
@@ -86,7 +86,7 @@ class Context:
     def opts(max_supernode_size=128, threads_per_source=0, sources_in_flight=0,
              supernodes=True, digests=True, l_row_stats=False, pattern=False,
              bu_alpha=0, bu_beta=0, heavy_row=0, bu_min_source=0, chunk_sources=0,
-             merge=True, cached_closures=0):
+             merge=True, cached_closures=0, global_bitmap=False):
         o = C.Opts()
         o.cached_closures = int(cached_closures)
         o.chunk_sources = int(chunk_sources)
@@ -99,7 +99,7 @@ class Context:
         o.sources_in_flight = int(sources_in_flight)
         o.flags = ((C.SUPERNODES if supernodes else 0) | (C.DIGESTS if digests else 0) |
                    (C.L_ROW_STATS if l_row_stats else 0) | (C.PATTERN if pattern else 0) |
-                   (0 if merge else C.NO_MERGE))
+                   (0 if merge else C.NO_MERGE) | (C.FORCE_GLOBAL_BITMAP if global_bitmap else 0))
         return o
 
     def autotune(self, mat, **kw):
@@ -120,6 +120,10 @@ class Context:
     def batch(self, mats, **kw):
         """Prepared graph-captured batch (see Batch)."""
         return Batch(self, mats, **kw)
+
+    def server(self, max_n, budget_bytes=0, **kw):
+        """Serving request loop (see Server)."""
+        return Server(self, max_n, budget_bytes, **kw)
 
     def factor_batch(self, mats, **kw):
         o = self.opts(**kw)
@@ -170,6 +174,89 @@ class Batch:
         if getattr(self, "_h", None):
             self.ctx._L.gsofa_batch_destroy(self._h)
             self._h = None
+
+
+class Server:
+    """Continuous-batching request loop: submit() queues a host CSR matrix and
+    returns a ticket; wait()/poll() hand out its Result.  The submitted
+    arrays are kept referenced here until their ticket completes (the library
+    reads them when it admits the request)."""
+
+    def __init__(self, ctx, max_n, budget_bytes=0, **kw):
+        self.ctx = ctx
+        self._L = ctx._L
+        o = ctx.opts(**kw)
+        h = ctypes.c_void_p()
+        ctx._check(self._L.gsofa_server_create(ctx.handle, ctypes.byref(o), int(max_n),
+                                               int(budget_bytes), ctypes.byref(h)), "server_create")
+        self._h = h
+        self._held = {}
+
+    def _raise(self, rc, what):
+        msg = self._L.gsofa_server_last_error(self._h).decode(errors="replace")
+        raise GsofaError(rc, "%s: %s" % (what, msg or self._L.gsofa_status_string(rc).decode()))
+
+    def submit(self, row_begin, row_end, col):
+        """Queue one request (rows col[row_begin[v]:row_end[v]]); returns its ticket."""
+        beg = np.ascontiguousarray(row_begin, dtype=np.int32)
+        end = np.ascontiguousarray(row_end, dtype=np.int32)
+        c = np.ascontiguousarray(col, dtype=np.int32)
+        t = ctypes.c_uint64()
+        rc = self._L.gsofa_server_submit(self._h, beg.shape[0], c.shape[0], _ptr(beg), _ptr(end),
+                                         _ptr(c), ctypes.byref(t))
+        if rc != C.OK:
+            self._raise(rc, "server_submit")
+        self._held[t.value] = (beg, end, c)
+        return t.value
+
+    def submit_rowptr(self, rowptr, col):
+        rowptr = np.asarray(rowptr)
+        return self.submit(rowptr[:-1], rowptr[1:], col)
+
+    def _finish(self, ticket, rc, h):
+        if rc == C.ERR_BUSY or rc == C.ERR_TIMEOUT:
+            return None
+        self._held.pop(ticket, None)
+        if rc != C.OK:
+            self._raise(rc, "ticket %d" % ticket)
+        return Result(self.ctx, h)
+
+    def poll(self, ticket):
+        """The Result if the ticket is complete, else None."""
+        h = ctypes.c_void_p()
+        return self._finish(ticket, self._L.gsofa_server_poll(self._h, int(ticket), ctypes.byref(h)), h)
+
+    def wait(self, ticket, timeout_ms=-1.0):
+        """Blocks until the ticket completes (None on timeout)."""
+        h = ctypes.c_void_p()
+        rc = self._L.gsofa_server_wait(self._h, int(ticket), float(timeout_ms), ctypes.byref(h))
+        return self._finish(ticket, rc, h)
+
+    def info(self, ticket):
+        i = C.TicketInfo()
+        rc = self._L.gsofa_server_ticket_info(self._h, int(ticket), ctypes.byref(i))
+        if rc != C.OK:
+            self._raise(rc, "ticket_info")
+        return {f: getattr(i, f) for f, _ in C.TicketInfo._fields_}
+
+    def stats(self):
+        st = C.ServerStats()
+        rc = self._L.gsofa_server_get_stats(self._h, ctypes.byref(st))
+        if rc != C.OK:
+            self._raise(rc, "server_stats")
+        return {f: getattr(st, f) for f, _ in C.ServerStats._fields_ if f != "reserved"}
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._L.gsofa_server_destroy(self._h)
+            self._h = None
+            self._held.clear()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
 
 
 class Matrix:

@@ -18,98 +18,14 @@
 #include <string>
 #include <vector>
 
-#include "../../include/gsofa.h"
-#include "gsofa_internal.h"
+#include "gsofa_host.h"
 
 using namespace gsofa;
-
-struct gsofa_ctx {
-    int device = 0;
-    int sm_count = 0;
-    int smem_optin = 0;
-    int smem_per_sm = 0;
-    size_t budget = 0;
-    size_t used = 0;
-    cudaStream_t own_stream = nullptr;
-    cudaStream_t stream = nullptr;
-    cudaMemPool_t pool = nullptr;
-    cudaEvent_t ev0 = nullptr, ev1 = nullptr, evt = nullptr;
-    std::recursive_mutex mu;
-    std::string err;
-    // autotuner choices per size class (log2 n, mean row length)
-    std::map<std::pair<int, int>, gsofa_opts> tuned;
-    // pinned staging
-    unsigned long long* h_counters = nullptr;  // CNT_SLOTS
-    int32_t* h_status = nullptr;
-    // grown workspace
-    void* queue = nullptr;
-    size_t queue_bytes = 0;
-    void* gbitmap = nullptr;
-    size_t gbitmap_bytes = 0;
-    void* gprev = nullptr;
-    size_t gprev_bytes = 0;
-    void* small = nullptr;  // work counter (8 B) + status (4 B)
-    void* scan_tmp = nullptr;
-    size_t scan_tmp_bytes = 0;
-};
-
-struct gsofa_matrix {
-    gsofa_ctx* ctx = nullptr;
-    int32_t n = 0;
-    int64_t nnz = 0;
-    int32_t* rowptr = nullptr;
-    int32_t* col = nullptr;
-    int32_t* trowptr = nullptr;
-    int32_t* tcol = nullptr;
-    int32_t* wdeg = nullptr;
-    size_t bytes = 0;
-};
-
-struct gsofa_result {
-    gsofa_ctx* ctx = nullptr;
-    int32_t n = 0;
-    uint32_t flags = 0;
-    int32_t mss = 128;
-    void* arena = nullptr;  // one device block holding every array below
-    size_t bytes = 0;
-    int32_t* nnz_u = nullptr;
-    int32_t* nz_row_u = nullptr;
-    uint64_t* dig_u = nullptr;
-    int32_t* nnz_lc = nullptr;
-    uint64_t* dig_lc = nullptr;
-    uint32_t* lmask = nullptr;
-    int32_t* nnz_lr = nullptr;
-    uint64_t* dig_lr = nullptr;
-    int8_t* sflags = nullptr;
-    unsigned long long* counters = nullptr;
-    // pattern (separate allocation, only with GSOFA_PATTERN)
-    void* parena = nullptr;
-    size_t pbytes = 0;
-    int64_t* uptr = nullptr;
-    int32_t* ucols = nullptr;
-    int64_t* lptr = nullptr;
-    int32_t* lrows = nullptr;
-    gsofa_counts counts{};
-    bool batch_owned = false;  // lives inside a gsofa_batch: not destroyed alone
-};
-
-struct gsofa_batch {
-    gsofa_ctx* ctx = nullptr;
-    int32_t count = 0;
-    gsofa_opts opts{};
-    std::vector<gsofa_result*> res;
-    void* ws = nullptr;  // private workspace (graph holds raw pointers into it)
-    size_t ws_bytes = 0;
-    unsigned long long* h_counters = nullptr;  // pinned, count * CNT_SLOTS
-    int32_t* h_status = nullptr;               // pinned
-    cudaEvent_t e0 = nullptr, et = nullptr, e1 = nullptr;
-    cudaGraph_t graph = nullptr;
-    cudaGraphExec_t exec = nullptr;
-    long long items = 0;
-};
+using namespace gsofa::host;
 
 // ---------------------------------------------------------------------------
-namespace {
+namespace gsofa {
+namespace host {
 
 int set_err(gsofa_ctx* ctx, int status, const char* fmt, ...) {
     if (ctx) {
@@ -133,7 +49,7 @@ int cuda_fail(gsofa_ctx* ctx, cudaError_t e, const char* where) {
         if (e_ != cudaSuccess) return cuda_fail(ctx, e_, #call); \
     } while (0)
 
-int dev_alloc(gsofa_ctx* ctx, size_t bytes, void** p) {
+int dev_alloc_on(gsofa_ctx* ctx, size_t bytes, void** p, cudaStream_t stream) {
     *p = nullptr;
     if (bytes == 0) return GSOFA_OK;
     bytes = (bytes + 255) & ~(size_t)255;
@@ -141,7 +57,7 @@ int dev_alloc(gsofa_ctx* ctx, size_t bytes, void** p) {
         return set_err(ctx, GSOFA_ERR_OOM_BUDGET,
                        "allocation of %zu bytes exceeds the budget (%zu of %zu bytes in use)",
                        bytes, ctx->used, ctx->budget);
-    cudaError_t e = cudaMallocFromPoolAsync(p, bytes, ctx->pool, ctx->stream);
+    cudaError_t e = cudaMallocFromPoolAsync(p, bytes, ctx->pool, stream);
     if (e != cudaSuccess) {
         *p = nullptr;
         return cuda_fail(ctx, e, "cudaMallocFromPoolAsync");
@@ -150,12 +66,18 @@ int dev_alloc(gsofa_ctx* ctx, size_t bytes, void** p) {
     return GSOFA_OK;
 }
 
-void dev_free(gsofa_ctx* ctx, void* p, size_t bytes) {
+void dev_free_on(gsofa_ctx* ctx, void* p, size_t bytes, cudaStream_t stream) {
     if (!p) return;
     bytes = (bytes + 255) & ~(size_t)255;
-    cudaFreeAsync(p, ctx->stream);
+    cudaFreeAsync(p, stream);
     ctx->used -= std::min(ctx->used, bytes);
 }
+
+int dev_alloc(gsofa_ctx* ctx, size_t bytes, void** p) {
+    return dev_alloc_on(ctx, bytes, p, ctx->stream);
+}
+
+void dev_free(gsofa_ctx* ctx, void* p, size_t bytes) { dev_free_on(ctx, p, bytes, ctx->stream); }
 
 // Grow-only workspace buffer.
 int ensure(gsofa_ctx* ctx, void** p, size_t* have, size_t need) {
@@ -172,14 +94,6 @@ int ensure(gsofa_ctx* ctx, void** p, size_t* have, size_t need) {
 size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
 
 long long bitmap_words(int32_t n) { return (((long long)n + 31) >> 5) + 6; }
-
-// Direction-switch and row-split defaults of the traversal (see
-// gsofa_kernels.cu); the autotuner overrides them per call.
-constexpr int kDefaultBuAlpha = 0;  // top-down only unless a caller asks
-constexpr int kDefaultBuBeta = 24;
-constexpr int kBuMinSource = 2048;
-constexpr int kDefaultHeavyRow = 64;
-constexpr int kDefaultRing = 32;
 
 // Default chunk (consecutive sources per work item): about four chunks per
 // CTA so the dynamic schedule can balance, between 16 and 512 sources.  Long
@@ -257,18 +171,12 @@ void result_free(gsofa_result* r) {
     delete r;
 }
 
-// Carve the per-row result arrays out of one arena.
-int result_alloc(gsofa_ctx* ctx, int32_t n, uint32_t flags, int32_t mss, gsofa_result** out) {
-    gsofa_result* r = new (std::nothrow) gsofa_result();
-    if (!r) return set_err(ctx, GSOFA_ERR_OOM_BUDGET, "host allocation failed");
-    r->ctx = ctx;
-    r->n = n;
-    r->flags = flags;
-    r->mss = mss;
+// Layout of a result arena: the per-row arrays of an n-row matrix.
+static size_t result_layout(int32_t n, uint32_t flags, size_t off[10]) {
     const size_t N = (size_t)std::max(n, 1);
     const bool dig = flags & GSOFA_DIGESTS;
     const bool lrow = flags & GSOFA_L_ROW_STATS;
-    size_t off[12], sz[12];
+    size_t sz[10];
     sz[0] = 4 * N;                       // nnz_u
     sz[1] = 4 * N;                       // nz_row_u
     sz[2] = dig ? 8 * N : 0;             // dig_u
@@ -284,7 +192,29 @@ int result_alloc(gsofa_ctx* ctx, int32_t n, uint32_t flags, int32_t mss, gsofa_r
         off[i] = total;
         total += align256(sz[i]);
     }
-    int rc = dev_alloc(ctx, total, &r->arena);
+    return total;
+}
+
+size_t result_bytes(int32_t n, uint32_t flags) {
+    size_t off[10];
+    return result_layout(n, flags, off);
+}
+
+// Carve the per-row result arrays out of one arena.
+int result_alloc_on(gsofa_ctx* ctx, int32_t n, uint32_t flags, int32_t mss, cudaStream_t stream,
+                    gsofa_result** out) {
+    gsofa_result* r = new (std::nothrow) gsofa_result();
+    if (!r) return set_err(ctx, GSOFA_ERR_OOM_BUDGET, "host allocation failed");
+    r->ctx = ctx;
+    r->n = n;
+    r->flags = flags;
+    r->mss = mss;
+    const size_t N = (size_t)std::max(n, 1);
+    const bool dig = flags & GSOFA_DIGESTS;
+    const bool lrow = flags & GSOFA_L_ROW_STATS;
+    size_t off[10];
+    const size_t total = result_layout(n, flags, off);
+    int rc = dev_alloc_on(ctx, total, &r->arena, stream);
     if (rc) {
         delete r;
         return rc;
@@ -304,17 +234,22 @@ int result_alloc(gsofa_ctx* ctx, int32_t n, uint32_t flags, int32_t mss, gsofa_r
     // zero the scatter targets, the counters and the flags
     cudaError_t e = cudaSuccess;
     if (lrow) {
-        e = cudaMemsetAsync(r->nnz_lr, 0, 4 * N, ctx->stream);
-        if (e == cudaSuccess) e = cudaMemsetAsync(r->dig_lr, 0, 8 * N, ctx->stream);
+        e = cudaMemsetAsync(r->nnz_lr, 0, 4 * N, stream);
+        if (e == cudaSuccess) e = cudaMemsetAsync(r->dig_lr, 0, 8 * N, stream);
     }
-    if (e == cudaSuccess) e = cudaMemsetAsync(r->counters, 0, 8 * CNT_SLOTS, ctx->stream);
-    if (e == cudaSuccess) e = cudaMemsetAsync(r->sflags, 0, N, ctx->stream);
+    if (e == cudaSuccess) e = cudaMemsetAsync(r->counters, 0, 8 * CNT_SLOTS, stream);
+    if (e == cudaSuccess) e = cudaMemsetAsync(r->sflags, 0, N, stream);
     if (e != cudaSuccess) {
-        result_free(r);
+        dev_free_on(ctx, r->arena, r->bytes, stream);
+        delete r;
         return cuda_fail(ctx, e, "result init");
     }
     *out = r;
     return GSOFA_OK;
+}
+
+int result_alloc(gsofa_ctx* ctx, int32_t n, uint32_t flags, int32_t mss, gsofa_result** out) {
+    return result_alloc_on(ctx, n, flags, mss, ctx->stream, out);
 }
 
 MatDesc make_desc(const gsofa_matrix* m, const gsofa_result* r, long long base) {
@@ -539,7 +474,8 @@ int64_t parse_ints(const std::string& s, size_t* pos, int64_t count, int32_t* ou
     return i;
 }
 
-}  // namespace
+}  // namespace host
+}  // namespace gsofa
 
 bool gsofa::matrix_view(const void* mat, MatrixView* out) {
     const gsofa_matrix* m = static_cast<const gsofa_matrix*>(mat);
@@ -552,6 +488,116 @@ bool gsofa::matrix_view(const void* mat, MatrixView* out) {
     out->tcol = m->tcol;
     out->wdeg = m->wdeg;
     return true;
+}
+
+void gsofa::host::ingest_bytes(int32_t n, int64_t nnz, size_t* kept, size_t* staging) {
+    // padded A: each row rounded up to 4 entries (at most 3n pads); A^T: the same bound
+    const size_t N1 = (size_t)n + 1;
+    const size_t PT = (size_t)std::max<int64_t>(nnz + 3ll * n, 4);
+    const size_t NW = (size_t)(((int64_t)n + 31) >> 5) + 1;
+    *kept = align256(4 * N1) * 2 + align256(4 * PT) * 2 + align256(4 * NW);
+    const size_t Nin = (size_t)std::max<int64_t>(nnz, 1);
+    *staging = align256(4 * N1) + align256(4 * Nin) + align256(4 * N1) * 3 +
+               align256(canonicalize_scan_bytes(n)) + 256;
+}
+
+int gsofa::host::ingest_csr(gsofa_ctx* ctx, cudaStream_t stream, int32_t* dstatus, int32_t n,
+                            int64_t nnz, const int32_t* row_begin, const int32_t* row_end,
+                            const int32_t* col, gsofa_matrix** out) {
+    *out = nullptr;
+    if (n < 0 || nnz < 0) return set_err(ctx, GSOFA_ERR_ARG, "negative n or nnz");
+    if (n > 0 && (!row_begin || !row_end)) return set_err(ctx, GSOFA_ERR_ARG, "null row arrays");
+    if (nnz > 0 && !col) return set_err(ctx, GSOFA_ERR_ARG, "null column array");
+    if (nnz > INT32_MAX) return set_err(ctx, GSOFA_ERR_UNSUPPORTED, "nnz above 2^31-1");
+    // host: padded row pointers of A.  Row v gets a multiple of 4 slots; the
+    // number of padding slots of row v sits in the low 2 bits of rp[v+1].
+    std::vector<int32_t> rp((size_t)n + 1);
+    int64_t acc = 0, real = 0;
+    rp[0] = 0;
+    for (int32_t v = 0; v < n; v++) {
+        const int64_t b = row_begin[v], e = row_end[v];
+        if (b < 0 || e < b || e > nnz)
+            return set_err(ctx, GSOFA_ERR_ARG, "row %d interval [%lld,%lld) outside [0,%lld)", v,
+                           (long long)b, (long long)e, (long long)nnz);
+        const int64_t d = e - b, pd = (d + 3) & ~(int64_t)3;
+        real += d;
+        acc += pd;
+        if (acc > INT32_MAX - 4 || real + 3ll * n > INT32_MAX - 4)
+            return set_err(ctx, GSOFA_ERR_UNSUPPORTED, "padded nnz above 2^31");
+        rp[(size_t)v + 1] = (int32_t)(acc | (pd - d));
+    }
+    const int64_t padded = acc;
+
+    gsofa_matrix* m = new (std::nothrow) gsofa_matrix();
+    if (!m) return set_err(ctx, GSOFA_ERR_OOM_BUDGET, "host allocation failed");
+    m->ctx = ctx;
+    m->n = n;
+    m->nnz = real;
+    const size_t N1 = (size_t)n + 1;
+    const size_t PA = (size_t)std::max<int64_t>(padded, 4);
+    const size_t PT = (size_t)std::max<int64_t>(real + 3ll * n, 4);  // bound for A^T
+    const size_t NW = (size_t)(((int64_t)n + 31) >> 5) + 1;
+    size_t total = align256(4 * N1) * 2 + align256(4 * PA) + align256(4 * PT) + align256(4 * NW);
+    void* blk = nullptr;
+    int rc = dev_alloc_on(ctx, total, &blk, stream);
+    if (rc) { delete m; return rc; }
+    m->bytes = total;
+    char* b = reinterpret_cast<char*>(blk);
+    m->rowptr = reinterpret_cast<int32_t*>(b);
+    m->trowptr = reinterpret_cast<int32_t*>(b + align256(4 * N1));
+    m->col = reinterpret_cast<int32_t*>(b + 2 * align256(4 * N1));
+    m->tcol = reinterpret_cast<int32_t*>(b + 2 * align256(4 * N1) + align256(4 * PA));
+    m->wdeg = reinterpret_cast<int32_t*>(b + 2 * align256(4 * N1) + align256(4 * PA) +
+                                         align256(4 * PT));
+
+    // staging: raw input (beg, col_in) and the transpose's counters
+    const size_t Nin = (size_t)std::max<int64_t>(nnz, 1);
+    size_t scan_bytes = canonicalize_scan_bytes(n);
+    size_t stage = align256(4 * N1) + align256(4 * Nin) + align256(4 * N1) * 3 +
+                   align256(scan_bytes) + 256;
+    void* sblk = nullptr;
+    rc = dev_alloc_on(ctx, stage, &sblk, stream);
+    if (rc) { dev_free_on(ctx, blk, total, stream); delete m; return rc; }
+    char* s = reinterpret_cast<char*>(sblk);
+    int32_t* dbeg = reinterpret_cast<int32_t*>(s);
+    s += align256(4 * N1);
+    int32_t* dcol_in = reinterpret_cast<int32_t*>(s);
+    s += align256(4 * Nin);
+    int32_t* tcount = reinterpret_cast<int32_t*>(s);
+    s += align256(4 * N1);
+    int32_t* tfill = reinterpret_cast<int32_t*>(s);
+    s += align256(4 * N1);
+    int32_t* tpad = reinterpret_cast<int32_t*>(s);
+    s += align256(4 * N1);
+    void* scan_tmp = s;
+
+    cudaError_t e = cudaSuccess;
+    auto cleanup = [&]() {
+        dev_free_on(ctx, sblk, stage, stream);
+        dev_free_on(ctx, blk, total, stream);
+        delete m;
+    };
+#define CKL(call)                                        \
+    do {                                                 \
+        e = (call);                                      \
+        if (e != cudaSuccess) { cleanup(); return cuda_fail(ctx, e, #call); } \
+    } while (0)
+    CKL(cudaMemcpyAsync(m->rowptr, rp.data(), 4 * N1, cudaMemcpyHostToDevice, stream));
+    if (n > 0) {
+        CKL(cudaMemcpyAsync(dbeg, row_begin, 4 * (size_t)n, cudaMemcpyHostToDevice, stream));
+    } else {
+        CKL(cudaMemsetAsync(m->trowptr, 0, 4, stream));
+    }
+    if (nnz > 0)
+        CKL(cudaMemcpyAsync(dcol_in, col, 4 * (size_t)nnz, cudaMemcpyHostToDevice, stream));
+    CKL(cudaMemsetAsync(tcount, 0, 4 * N1, stream));
+    CKL(cudaMemsetAsync(tfill, 0, 4 * N1, stream));
+    CKL(launch_canonicalize(n, nnz, dbeg, dcol_in, m->rowptr, m->col, tcount, tpad, m->trowptr,
+                            m->tcol, tfill, m->wdeg, scan_tmp, scan_bytes, dstatus, stream));
+#undef CKL
+    dev_free_on(ctx, sblk, stage, stream);  // stream-ordered: after the build
+    *out = m;
+    return GSOFA_OK;
 }
 
 // ============================================================================
@@ -689,106 +735,18 @@ int gsofa_load_csr(gsofa_ctx* ctx, int32_t n, int64_t nnz, const int32_t* row_be
     if (!ctx || !out) return GSOFA_ERR_ARG;
     *out = nullptr;
     std::lock_guard<std::recursive_mutex> g(ctx->mu);
-    if (n < 0 || nnz < 0) return set_err(ctx, GSOFA_ERR_ARG, "negative n or nnz");
-    if (n > 0 && (!row_begin || !row_end)) return set_err(ctx, GSOFA_ERR_ARG, "null row arrays");
-    if (nnz > 0 && !col) return set_err(ctx, GSOFA_ERR_ARG, "null column array");
-    if (nnz > INT32_MAX) return set_err(ctx, GSOFA_ERR_UNSUPPORTED, "nnz above 2^31-1");
     if (cudaSetDevice(ctx->device) != cudaSuccess) return set_err(ctx, GSOFA_ERR_CUDA, "cudaSetDevice");
-    // host: padded row pointers of A.  Row v gets a multiple of 4 slots; the
-    // number of padding slots of row v sits in the low 2 bits of rp[v+1].
-    std::vector<int32_t> rp((size_t)n + 1);
-    int64_t acc = 0, real = 0;
-    rp[0] = 0;
-    for (int32_t v = 0; v < n; v++) {
-        const int64_t b = row_begin[v], e = row_end[v];
-        if (b < 0 || e < b || e > nnz)
-            return set_err(ctx, GSOFA_ERR_ARG, "row %d interval [%lld,%lld) outside [0,%lld)", v,
-                           (long long)b, (long long)e, (long long)nnz);
-        const int64_t d = e - b, pd = (d + 3) & ~(int64_t)3;
-        real += d;
-        acc += pd;
-        if (acc > INT32_MAX - 4 || real + 3ll * n > INT32_MAX - 4)
-            return set_err(ctx, GSOFA_ERR_UNSUPPORTED, "padded nnz above 2^31");
-        rp[(size_t)v + 1] = (int32_t)(acc | (pd - d));
-    }
-    const int64_t padded = acc;
-
-    gsofa_matrix* m = new (std::nothrow) gsofa_matrix();
-    if (!m) return set_err(ctx, GSOFA_ERR_OOM_BUDGET, "host allocation failed");
-    m->ctx = ctx;
-    m->n = n;
-    m->nnz = real;
-    const size_t N1 = (size_t)n + 1;
-    const size_t PA = (size_t)std::max<int64_t>(padded, 4);
-    const size_t PT = (size_t)std::max<int64_t>(real + 3ll * n, 4);  // bound for A^T
-    const size_t NW = (size_t)(((int64_t)n + 31) >> 5) + 1;
-    size_t total = align256(4 * N1) * 2 + align256(4 * PA) + align256(4 * PT) + align256(4 * NW);
-    void* blk = nullptr;
-    int rc = dev_alloc(ctx, total, &blk);
-    if (rc) { delete m; return rc; }
-    m->bytes = total;
-    char* b = reinterpret_cast<char*>(blk);
-    m->rowptr = reinterpret_cast<int32_t*>(b);
-    m->trowptr = reinterpret_cast<int32_t*>(b + align256(4 * N1));
-    m->col = reinterpret_cast<int32_t*>(b + 2 * align256(4 * N1));
-    m->tcol = reinterpret_cast<int32_t*>(b + 2 * align256(4 * N1) + align256(4 * PA));
-    m->wdeg = reinterpret_cast<int32_t*>(b + 2 * align256(4 * N1) + align256(4 * PA) +
-                                         align256(4 * PT));
-
-    // staging: raw input (beg, col_in) and the transpose's counters
-    const size_t Nin = (size_t)std::max<int64_t>(nnz, 1);
-    size_t scan_bytes = canonicalize_scan_bytes(n);
-    size_t stage = align256(4 * N1) + align256(4 * Nin) + align256(4 * N1) * 3 +
-                   align256(scan_bytes) + 256;
-    void* sblk = nullptr;
-    rc = dev_alloc(ctx, stage, &sblk);
-    if (rc) { dev_free(ctx, blk, total); delete m; return rc; }
-    char* s = reinterpret_cast<char*>(sblk);
-    int32_t* dbeg = reinterpret_cast<int32_t*>(s);
-    s += align256(4 * N1);
-    int32_t* dcol_in = reinterpret_cast<int32_t*>(s);
-    s += align256(4 * Nin);
-    int32_t* tcount = reinterpret_cast<int32_t*>(s);
-    s += align256(4 * N1);
-    int32_t* tfill = reinterpret_cast<int32_t*>(s);
-    s += align256(4 * N1);
-    int32_t* tpad = reinterpret_cast<int32_t*>(s);
-    s += align256(4 * N1);
-    void* scan_tmp = s;
-
     unsigned long long* wc = nullptr;
     int32_t* dstatus = work_counter_status(ctx, &wc);
-    cudaError_t e = cudaSuccess;
-    auto cleanup = [&]() {
-        dev_free(ctx, sblk, stage);
-        dev_free(ctx, blk, total);
-        delete m;
-    };
-#define CKL(call)                                        \
-    do {                                                 \
-        e = (call);                                      \
-        if (e != cudaSuccess) { cleanup(); return cuda_fail(ctx, e, #call); } \
-    } while (0)
-    CKL(cudaMemsetAsync(ctx->small, 0, 128, ctx->stream));
-    CKL(cudaMemcpyAsync(m->rowptr, rp.data(), 4 * N1, cudaMemcpyHostToDevice, ctx->stream));
-    if (n > 0) {
-        CKL(cudaMemcpyAsync(dbeg, row_begin, 4 * (size_t)n, cudaMemcpyHostToDevice, ctx->stream));
-    } else {
-        CKL(cudaMemsetAsync(m->trowptr, 0, 4, ctx->stream));
-    }
-    if (nnz > 0)
-        CKL(cudaMemcpyAsync(dcol_in, col, 4 * (size_t)nnz, cudaMemcpyHostToDevice, ctx->stream));
-    CKL(cudaMemsetAsync(tcount, 0, 4 * N1, ctx->stream));
-    CKL(cudaMemsetAsync(tfill, 0, 4 * N1, ctx->stream));
-    CKL(launch_canonicalize(n, nnz, dbeg, dcol_in, m->rowptr, m->col, tcount, tpad, m->trowptr,
-                            m->tcol, tfill, m->wdeg, scan_tmp, scan_bytes, dstatus, ctx->stream));
-    CKL(cudaMemcpyAsync(ctx->h_status, dstatus, 4, cudaMemcpyDeviceToHost, ctx->stream));
-    CKL(cudaStreamSynchronize(ctx->stream));
-#undef CKL
-    dev_free(ctx, sblk, stage);
-    rc = check_status(ctx);
+    CK(cudaMemsetAsync(ctx->small, 0, 128, ctx->stream));
+    gsofa_matrix* m = nullptr;
+    int rc = ingest_csr(ctx, ctx->stream, dstatus, n, nnz, row_begin, row_end, col, &m);
+    if (rc) return rc;
+    cudaError_t e = cudaMemcpyAsync(ctx->h_status, dstatus, 4, cudaMemcpyDeviceToHost, ctx->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+    rc = e != cudaSuccess ? cuda_fail(ctx, e, "load") : check_status(ctx);
     if (rc) {
-        dev_free(ctx, blk, total);
+        dev_free(ctx, m->rowptr, m->bytes);
         delete m;
         return rc;
     }

@@ -1,0 +1,135 @@
+// Host-side handle structures and helpers shared by the translation units
+// of libgsofa.so (gsofa_capi.cpp: the C-ABI; gsofa_server.cpp: the request
+// loop).  Not installed.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <map>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/gsofa.h"
+#include "gsofa_internal.h"
+
+struct gsofa_ctx {
+    int device = 0;
+    int sm_count = 0;
+    int smem_optin = 0;
+    int smem_per_sm = 0;
+    size_t budget = 0;
+    size_t used = 0;
+    cudaStream_t own_stream = nullptr;
+    cudaStream_t stream = nullptr;
+    cudaMemPool_t pool = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr, evt = nullptr;
+    std::recursive_mutex mu;
+    std::string err;
+    // autotuner choices per size class (log2 n, mean row length)
+    std::map<std::pair<int, int>, gsofa_opts> tuned;
+    // pinned staging
+    unsigned long long* h_counters = nullptr;  // CNT_SLOTS
+    int32_t* h_status = nullptr;
+    // grown workspace
+    void* queue = nullptr;
+    size_t queue_bytes = 0;
+    void* gbitmap = nullptr;
+    size_t gbitmap_bytes = 0;
+    void* gprev = nullptr;
+    size_t gprev_bytes = 0;
+    void* small = nullptr;  // work counter (8 B) + status (4 B)
+    void* scan_tmp = nullptr;
+    size_t scan_tmp_bytes = 0;
+};
+
+struct gsofa_matrix {
+    gsofa_ctx* ctx = nullptr;
+    int32_t n = 0;
+    int64_t nnz = 0;
+    int32_t* rowptr = nullptr;
+    int32_t* col = nullptr;
+    int32_t* trowptr = nullptr;
+    int32_t* tcol = nullptr;
+    int32_t* wdeg = nullptr;
+    size_t bytes = 0;
+};
+
+struct gsofa_result {
+    gsofa_ctx* ctx = nullptr;
+    int32_t n = 0;
+    uint32_t flags = 0;
+    int32_t mss = 128;
+    void* arena = nullptr;  // one device block holding every array below
+    size_t bytes = 0;
+    int32_t* nnz_u = nullptr;
+    int32_t* nz_row_u = nullptr;
+    uint64_t* dig_u = nullptr;
+    int32_t* nnz_lc = nullptr;
+    uint64_t* dig_lc = nullptr;
+    uint32_t* lmask = nullptr;
+    int32_t* nnz_lr = nullptr;
+    uint64_t* dig_lr = nullptr;
+    int8_t* sflags = nullptr;
+    unsigned long long* counters = nullptr;
+    // pattern (separate allocation, only with GSOFA_PATTERN)
+    void* parena = nullptr;
+    size_t pbytes = 0;
+    int64_t* uptr = nullptr;
+    int32_t* ucols = nullptr;
+    int64_t* lptr = nullptr;
+    int32_t* lrows = nullptr;
+    gsofa_counts counts{};
+    bool batch_owned = false;  // lives inside a gsofa_batch: not destroyed alone
+};
+
+struct gsofa_batch {
+    gsofa_ctx* ctx = nullptr;
+    int32_t count = 0;
+    gsofa_opts opts{};
+    std::vector<gsofa_result*> res;
+    void* ws = nullptr;  // private workspace (graph holds raw pointers into it)
+    size_t ws_bytes = 0;
+    unsigned long long* h_counters = nullptr;  // pinned, count * CNT_SLOTS
+    int32_t* h_status = nullptr;               // pinned
+    cudaEvent_t e0 = nullptr, et = nullptr, e1 = nullptr;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    long long items = 0;
+};
+
+namespace gsofa {
+namespace host {
+
+int set_err(gsofa_ctx* ctx, int status, const char* fmt, ...);
+int cuda_fail(gsofa_ctx* ctx, cudaError_t e, const char* where);
+// Pool allocation with budget accounting, ordered on `stream`; the caller
+// holds ctx->mu.
+int dev_alloc_on(gsofa_ctx* ctx, size_t bytes, void** p, cudaStream_t stream);
+void dev_free_on(gsofa_ctx* ctx, void* p, size_t bytes, cudaStream_t stream);
+size_t align256(size_t x);
+long long default_chunk(long long total_sources, int grid);
+int default_block(int32_t nmax, int smem_per_sm);
+// Result arrays of an n-row matrix, zero-initialised on `stream`.
+int result_alloc_on(gsofa_ctx* ctx, int32_t n, uint32_t flags, int32_t mss, cudaStream_t stream,
+                    gsofa_result** out);
+void result_free(gsofa_result* r);
+MatDesc make_desc(const gsofa_matrix* m, const gsofa_result* r, long long base);
+// Validates the row intervals on the host, then queues the upload and the
+// padded-CSR build of A and A^T on `stream` without waiting.  Column ids
+// outside [0, n) are reported in *dstatus (DEV_ERR_COL_RANGE) when the
+// stream reaches the build.  The caller holds ctx->mu.
+int ingest_csr(gsofa_ctx* ctx, cudaStream_t stream, int32_t* dstatus, int32_t n, int64_t nnz,
+               const int32_t* row_begin, const int32_t* row_end, const int32_t* col,
+               gsofa_matrix** out);
+// Device bytes ingest_csr holds for a matrix (kept) and while it runs (staging).
+void ingest_bytes(int32_t n, int64_t nnz, size_t* kept, size_t* staging);
+size_t result_bytes(int32_t n, uint32_t flags);
+
+constexpr int kDefaultBuAlpha = 0;  // top-down only unless a caller asks
+constexpr int kDefaultBuBeta = 24;
+constexpr int kBuMinSource = 2048;
+constexpr int kDefaultHeavyRow = 64;
+constexpr int kDefaultRing = 32;
+
+}  // namespace host
+}  // namespace gsofa

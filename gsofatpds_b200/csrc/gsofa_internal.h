@@ -49,6 +49,46 @@ struct MatDesc {
     const int64_t* lptr;        // pattern pass: L column pointers (n+1) or null
     int32_t* lrows;
     long long item_base;        // first work item of this matrix
+    // serving only (zero elsewhere)
+    long long n_items;          // work items of this request
+    unsigned long long seq;     // request number (claim word tag, done flag value)
+    int32_t chunk;              // consecutive sources per work item
+    int32_t slot;               // slot of the serving tables
+};
+
+// The serving kernel's view of the request loop.  Each admitted request
+// owns a slot: its descriptor, a claim word (request number << 32 | items
+// claimed) and a finished-items counter.  The host publishes a request by
+// writing its claim word (request number, 0) with a stream-ordered copy after
+// the request's build and descriptor, and lists (slot, request number) in a
+// device table it rewrites with small copies.  A CTA picks the listed request
+// with the fewest unclaimed items and claims one with compare-and-swap; a
+// claim only succeeds while the word still carries the entry's request
+// number, so stale or torn list entries are harmless.  The CTA that finishes
+// a request's last item writes the request number to done_flags[slot]
+// (mapped host memory, the one place the kernel touches host memory).
+// Every wait is bounded: a CTA that finds nothing to claim for idle_ns (or
+// max_idle_polls polls) exits, which also returns its SM to other work.
+struct ServeLaunch {
+    unsigned long long* claim;            // per slot
+    const unsigned long long* list;       // (slot << 32) | request number
+    const int32_t* ctrl;                  // [0] exit when idle, [1] take no more items, [2] list entries
+    unsigned int* rr;                     // rotating start of the list scan (tie order)
+    const MatDesc* slots;                 // one descriptor per slot
+    unsigned long long* items_done;       // per slot: finished items
+    const int32_t* slot_status;           // per slot: ingest error word
+    unsigned long long* done_flags;       // mapped host memory, per slot
+    int32_t nslots;
+    long long smem_words;                 // bitmap words that fit in shared memory
+    long long max_idle_polls;
+    long long idle_ns;
+    // per-CTA workspace slots (queue, closure ring, global bitmap): several
+    // launches may run at once, so a CTA takes a free slot when it starts
+    // (bit set in cta_slots) instead of using its block index, and returns
+    // it when it exits; a CTA that finds none exits at once
+    unsigned int* cta_slots;
+    int32_t n_cta_slots;
+    int* alive;                           // CTAs holding a slot
 };
 
 struct TraverseLaunch {
@@ -71,6 +111,7 @@ struct TraverseLaunch {
     int bu_beta;                // bottom-up -> top-down when found*beta < unseen
     int bu_min_src;             // sources below this id stay top-down
     int heavy_len;              // padded rows longer than this are walked by a whole warp
+    ServeLaunch serve;          // serving kernel only
 };
 
 // Launch helpers (gsofa_kernels.cu).  All asynchronous on `stream`.
@@ -79,6 +120,12 @@ int traverse_block_sizes(int* sizes, int max_sizes);
 int traverse_occupancy(int block, bool smem_bitmap, size_t smem_bytes);
 cudaError_t launch_traverse(const TraverseLaunch& L, int block, int grid, bool smem_bitmap,
                             size_t smem_bytes, cudaStream_t stream);
+// The serving kernel: bitmaps of up to L.serve.smem_words words in shared
+// memory (smem_bytes), wider ones in L.gbitmap.
+int serve_occupancy(int block, size_t smem_bytes);
+cudaError_t launch_serve(const TraverseLaunch& L, int block, int grid, size_t smem_bytes,
+                         cudaStream_t stream);
+
 // Builds the padded CSR of A (row pointers rp precomputed on the host, with
 // pad counts in their low 2 bits) and of A^T.
 cudaError_t launch_canonicalize(int32_t n, long long nnz_in, const int32_t* beg,

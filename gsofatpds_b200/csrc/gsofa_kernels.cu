@@ -64,13 +64,26 @@ __device__ __forceinline__ uint32_t ld_vol(const uint32_t* p) {
     return *reinterpret_cast<const volatile uint32_t*>(p);
 }
 
+// Loads of matrix data.  CG = false: the read-only path (L1-cached), valid
+// because nothing writes a matrix while a launch reads it.  CG = true (the
+// serving kernel): L2 only.  A serving launch outlives the matrices it reads;
+// their memory is freed and reused for later requests while it runs, so a
+// line it once cached in L1 could be stale.
+template <bool CG>
+__device__ __forceinline__ int ld_i32(const int32_t* p) {
+    return CG ? __ldcg(p) : __ldg(p);
+}
+
+template <bool CG>
 __device__ __forceinline__ int4 ld_row4(const int32_t* p) {
-    return __ldg(reinterpret_cast<const int4*>(p));
+    const int4* q = reinterpret_cast<const int4*>(p);
+    return CG ? __ldcg(q) : __ldg(q);
 }
 
 // Original (unpadded) length of row v of a padded graph.
+template <bool CG>
 __device__ __forceinline__ int row_degree(const int32_t* rp, int v) {
-    const int a = __ldg(rp + v), b = __ldg(rp + v + 1);
+    const int a = ld_i32<CG>(rp + v), b = ld_i32<CG>(rp + v + 1);
     return (b & ~3) - (a & ~3) - (b & 3);
 }
 
@@ -85,6 +98,9 @@ struct TraverseSmem {
     int pushed;       // ids a merge appended to the queue
     unsigned pending; // cached sources a merge set (slots), for the next decision
     unsigned reached[3];  // per level (rotating): cached sources first reached
+    int mi;               // matrix of the current item
+    int skip;             // the current item's matrix failed ingest: count it only
+    int cta;              // workspace slot (serving) or block index
 };
 
 // Bitmap words of a matrix of order n: n bits plus zero padding read by the
@@ -203,7 +219,7 @@ __device__ __forceinline__ unsigned td_edge4(const Src& S, int v, const int4& e,
 // One top-down level: expand queue[lb, le), append new vertices after le.
 // After a merge, vertices inside the merged closure (and the source itself)
 // are skipped: their reach is already in the bitmap.
-template <int BLOCK>
+template <int BLOCK, bool CG>
 __device__ __forceinline__ void td_level(const Src& S, int32_t* q, long long qcap, long long lb,
                                          long long le, int* cnt, int32_t* status, int heavy_len,
                                          uint32_t& raw, uint32_t& orig, uint32_t& trav) {
@@ -222,7 +238,7 @@ __device__ __forceinline__ void td_level(const Src& S, int32_t* q, long long qca
             bool skip = false;
             if (S.merged_mask) skip = v == S.src || covered(S, S.top, v);
             if (!skip) {
-                const int r0 = __ldg(S.rp + v), r1 = __ldg(S.rp + v + 1);
+                const int r0 = ld_i32<CG>(S.rp + v), r1 = ld_i32<CG>(S.rp + v + 1);
                 s0 = r0 & ~3;
                 plen = (r1 & ~3) - s0;
                 trav += (uint32_t)plen;
@@ -240,7 +256,7 @@ __device__ __forceinline__ void td_level(const Src& S, int32_t* q, long long qca
             const int hv = __shfl_sync(FULL_MASK, v, l);
             for (int k0 = 0; k0 < hl; k0 += 128) {
                 const int k = k0 + 4 * lane;
-                const int4 e = k < hl ? ld_row4(S.cl + hb + k) : idle;
+                const int4 e = k < hl ? ld_row4<CG>(S.cl + hb + k) : idle;
                 const unsigned f = td_edge4(S, hv, e, raw, orig);
                 push4(q, qcap, le, cnt, status, lane, e, f);
             }
@@ -250,7 +266,7 @@ __device__ __forceinline__ void td_level(const Src& S, int32_t* q, long long qca
         const int its = plen >> 2;
         const int maxit = __reduce_max_sync(FULL_MASK, its);
         for (int it = 0; it < maxit; it++) {
-            const int4 e = it < its ? ld_row4(S.cl + s0 + 4 * it) : idle;
+            const int4 e = it < its ? ld_row4<CG>(S.cl + s0 + 4 * it) : idle;
             const unsigned f = td_edge4(S, v, e, raw, orig);
             push4(q, qcap, le, cnt, status, lane, e, f);
         }
@@ -264,7 +280,7 @@ __device__ __forceinline__ bool seen_le_src(const Src& S, int p) {
 // Bottom-up sweep.  upper == false: unseen u < src become seen (and queued)
 // when an in-neighbour p <= src is seen.  upper == true: unmarked w in
 // (src, n) are marked when an in-neighbour p <= src is seen.
-template <int BLOCK>
+template <int BLOCK, bool CG>
 __device__ __forceinline__ void bu_sweep(const Src& S, bool upper, int32_t* q, long long qcap,
                                          long long le, int* cnt, int32_t* status, uint32_t& trav) {
     constexpr int NW = BLOCK / 32;
@@ -281,10 +297,10 @@ __device__ __forceinline__ void bu_sweep(const Src& S, bool upper, int32_t* q, l
         if (!__any_sync(FULL_MASK, need)) continue;
         bool found = false;
         if (need) {
-            const int a0 = __ldg(S.irp + u), a1 = __ldg(S.irp + u + 1);
+            const int a0 = ld_i32<CG>(S.irp + u), a1 = ld_i32<CG>(S.irp + u + 1);
             const int ib = a0 & ~3, ie = a1 & ~3;
             for (int j = ib; j < ie; j += 4) {
-                const int4 p = ld_row4(S.icl + j);
+                const int4 p = ld_row4<CG>(S.icl + j);
                 trav += 4;
                 if (seen_le_src(S, p.x) || seen_le_src(S, p.y) || seen_le_src(S, p.z) ||
                     seen_le_src(S, p.w)) {
@@ -392,41 +408,225 @@ __device__ __forceinline__ uint32_t merge_reached(const Src& S, uint32_t reached
     return mm;
 }
 
-template <int BLOCK, bool SMEM_BM>
+__device__ __forceinline__ unsigned long long ld_vol64(const unsigned long long* p) {
+    return *reinterpret_cast<const volatile unsigned long long*>(p);
+}
+
+__device__ __forceinline__ int ld_vol_i32(const int32_t* p) {
+    return *reinterpret_cast<const volatile int32_t*>(p);
+}
+
+__device__ __forceinline__ unsigned long long global_ns() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+// Serving, called by all 32 lanes of warp 0: claims a work item of any
+// published request.  Each lane checks one list entry (rotating start); the
+// claimable entry with the fewest unclaimed items is taken with
+// compare-and-swap on its claim word.  Returns false (in every
+// lane) when the host says to take no more items (ctrl[1]), when nothing is
+// claimable and the host asks idle CTAs to exit (ctrl[0]), after idle_ns of
+// finding nothing, or after max_idle_polls polls.
+__device__ bool serve_claim(const TraverseLaunch& P, int* slot_out, long long* item_out) {
+    const ServeLaunch& V = P.serve;
+    const int lane = threadIdx.x & 31;
+    unsigned ns = 32;
+    const unsigned long long t0 = global_ns();
+    for (long long polls = 0; polls < V.max_idle_polls; polls++) {
+        int c0 = 0, c1 = 0, n = 0;
+        unsigned r = 0;
+        if (lane == 0) {
+            c1 = ld_vol_i32(V.ctrl + 1);
+            c0 = ld_vol_i32(V.ctrl);
+            n = min(ld_vol_i32(V.ctrl + 2), V.nslots);
+            if (!c1 && n > 0) r = atomicAdd(V.rr, 1u);
+        }
+        c0 = __shfl_sync(FULL_MASK, c0, 0);
+        c1 = __shfl_sync(FULL_MASK, c1, 0);
+        n = __shfl_sync(FULL_MASK, n, 0);
+        r = __shfl_sync(FULL_MASK, r, 0);
+        if (c1) return false;
+        for (int base = 0; base < n; base += 32) {
+            const int k = base + lane;
+            bool ok = false;
+            int slot = -1;
+            unsigned seq = 0;
+            unsigned long long v = 0;
+            long long nit = 0;
+            if (k < n) {
+                const unsigned long long e = ld_vol64(V.list + (r + (unsigned)k) % (unsigned)n);
+                slot = (int)(e >> 32);
+                seq = (unsigned)e;
+                if (slot >= 0 && slot < V.nslots) {
+                    v = ld_vol64(V.claim + slot);
+                    if ((unsigned)(v >> 32) == seq) {
+                        __threadfence();  // the descriptor was written before the claim word
+                        nit = __ldcg(&V.slots[slot].n_items);
+                        ok = (long long)(v & 0xffffffffull) < nit;
+                    }
+                }
+            }
+            // shortest remaining work first (fewest unclaimed items), ties in
+            // rotation order: small requests overtake large ones item by item
+            unsigned rem = 0xffffffffu;
+            if (ok) rem = (unsigned)min(nit - (long long)(v & 0xffffffffull), 0xfffffffell);
+            for (int round = 0; round < 32; round++) {
+                const unsigned best = __reduce_min_sync(FULL_MASK, rem);
+                if (best == 0xffffffffu) break;
+                const int l = __ffs(__ballot_sync(FULL_MASK, rem == best)) - 1;
+                int got = 0;
+                long long it = 0;
+                if (lane == l) {
+                    for (int tries = 0; tries < 256; tries++) {
+                        if ((unsigned)(v >> 32) != seq || (long long)(v & 0xffffffffull) >= nit) break;
+                        const unsigned long long old = atomicCAS(V.claim + slot, v, v + 1ull);
+                        if (old == v) {
+                            got = 1;
+                            it = (long long)(v & 0xffffffffull);
+                            break;
+                        }
+                        v = old;
+                    }
+                    rem = 0xffffffffu;  // taken or gone: this entry is done
+                }
+                if (__shfl_sync(FULL_MASK, got, l)) {
+                    *slot_out = __shfl_sync(FULL_MASK, slot, l);
+                    *item_out = __shfl_sync(FULL_MASK, it, l);
+                    return true;
+                }
+            }
+        }
+        if (c0) return false;
+        if (global_ns() - t0 > (unsigned long long)V.idle_ns) return false;
+        __nanosleep(ns);
+        if (ns < 2048) ns <<= 1;
+    }
+    return false;
+}
+
+// Serving: takes a free per-CTA workspace slot, or returns -1.
+__device__ int take_cta_slot(const ServeLaunch& V) {
+    const int nw = (V.n_cta_slots + 31) >> 5;
+    for (int w = 0; w < nw; w++) {
+        unsigned v = ld_vol_i32(reinterpret_cast<const int32_t*>(V.cta_slots + w));
+        for (int tries = 0; tries < 64 && ~v; tries++) {
+            const int b = __ffs(~v) - 1;
+            if (w * 32 + b >= V.n_cta_slots) break;
+            const unsigned old = atomicOr(V.cta_slots + w, 1u << b);
+            if (!(old & (1u << b))) {
+                atomicAdd(V.alive, 1);
+                __threadfence();
+                return w * 32 + b;
+            }
+            v = old | (1u << b);
+        }
+    }
+    return -1;
+}
+
+// Thread 0 copies a matrix descriptor to shared memory (through L2 when it
+// may have been rewritten since the launch began).
+template <bool CG>
+__device__ __forceinline__ void copy_desc(MatDesc* dst, const MatDesc* src) {
+    static_assert(sizeof(MatDesc) % 8 == 0, "descriptor copied in 8-byte words");
+    const unsigned long long* a = reinterpret_cast<const unsigned long long*>(src);
+    unsigned long long* b = reinterpret_cast<unsigned long long*>(dst);
+#pragma unroll
+    for (int k = 0; k < (int)(sizeof(MatDesc) / 8); k++) b[k] = CG ? __ldcg(a + k) : a[k];
+}
+
+__device__ __forceinline__ void flush_counters(unsigned long long* c, unsigned long long* acc) {
+    atomicAdd(&c[CNT_FILLS], acc[0]);
+    atomicAdd(&c[CNT_EDGES_ALG], acc[1]);
+    atomicAdd(&c[CNT_VERTS_ALG], acc[2]);
+    atomicAdd(&c[CNT_EDGES_TRAV], acc[3]);
+    atomicAdd(&c[CNT_NNZ_U], acc[4]);
+    atomicAdd(&c[CNT_NNZ_L], acc[5]);
+    for (int j = 0; j < 6; j++) acc[j] = 0;
+}
+
+// MODE 0: each CTA's bitmap in global memory; 1: in shared memory;
+// 2: serving -- items come from the requests the request loop publishes, and an
+// item's bitmap sits in shared memory when the matrix fits, else in global
+// memory (kept zero between items by the census, zeroed by the host once).
+template <int BLOCK, int MODE>
 __global__ void __launch_bounds__(BLOCK, 1024 / BLOCK) traverse_kernel(TraverseLaunch P) {
     extern __shared__ uint4 dyn_smem[];
     __shared__ TraverseSmem<BLOCK> SM;
+    __shared__ MatDesc SD;  // the current item's matrix
+    constexpr bool CG = MODE == 2;
     constexpr int NW = BLOCK / 32;
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
-    uint32_t* bm = SMEM_BM ? reinterpret_cast<uint32_t*>(dyn_smem)
-                           : P.gbitmap + (long long)blockIdx.x * P.bitmap_words;
-    uint32_t* ring_base = P.gprev + (long long)blockIdx.x * P.ring * P.bitmap_words;
-    int32_t* q = P.queue + (long long)blockIdx.x * P.queue_stride;
+    if constexpr (MODE == 2) {
+        if (threadIdx.x == 0) SM.cta = take_cta_slot(P.serve);
+        __syncthreads();
+        if (SM.cta < 0) return;  // every workspace slot is taken
+    } else if (threadIdx.x == 0) {
+        SM.cta = blockIdx.x;
+    }
+    const long long cta = MODE == 2 ? SM.cta : blockIdx.x;
+    uint32_t* const sbm = reinterpret_cast<uint32_t*>(dyn_smem);
+    uint32_t* const gbm = MODE == 1 ? nullptr : P.gbitmap + cta * P.bitmap_words;
+    uint32_t* bm = MODE == 1 ? sbm : gbm;
+    uint32_t* ring_base = P.gprev + cta * P.ring * P.bitmap_words;
+    int32_t* q = P.queue + cta * P.queue_stride;
     const long long qcap = P.queue_stride;
 
-    for (long long i = threadIdx.x; i < P.bitmap_words; i += BLOCK) bm[i] = 0u;
+    if constexpr (MODE == 2) {
+        for (long long i = threadIdx.x; i < P.serve.smem_words; i += BLOCK) sbm[i] = 0u;
+    } else {
+        for (long long i = threadIdx.x; i < P.bitmap_words; i += BLOCK) bm[i] = 0u;
+    }
 
     // thread 0 accumulates per-matrix counters and flushes on matrix change
+    // (serving: after every item)
     int acc_mat = -1;
     unsigned long long acc[6] = {0, 0, 0, 0, 0, 0};
+    const long long stride = P.sample_stride > 1 ? P.sample_stride : 1;
 
     for (;;) {
-        if (threadIdx.x == 0) SM.item = (long long)atomicAdd(P.work_counter, 1ull);
+        if constexpr (MODE == 2) {
+            if (warp == 0) {
+                int slot = 0;
+                long long it = -1;
+                const bool got = serve_claim(P, &slot, &it);
+                if (lane == 0) {
+                    if (got) {
+                        copy_desc<true>(&SD, P.serve.slots + slot);
+                        SM.skip = __ldcg(P.serve.slot_status + slot) != 0;  // ingest failed
+                    }
+                    SM.item = got ? it : -1;
+                }
+            }
+        } else if (threadIdx.x == 0) {
+            const unsigned long long c = atomicAdd(P.work_counter, 1ull);
+            const long long it = (long long)c < P.total_items ? (long long)c : -1;
+            if (it >= 0) {
+                SM.mi = find_matrix(P.mats, P.nmats, it * stride);
+                copy_desc<false>(&SD, P.mats + SM.mi);
+                SM.skip = 0;
+            }
+            SM.item = it;
+        }
         __syncthreads();
-        if (SM.item >= P.total_items) break;
-        const long long item = SM.item * (P.sample_stride > 1 ? P.sample_stride : 1);
-        const int mi = find_matrix(P.mats, P.nmats, item);
-        const MatDesc& M = P.mats[mi];
+        if (SM.item < 0) break;
+        const MatDesc& M = SD;
+        const int mi = MODE == 2 ? 0 : SM.mi;
+        const long long item = MODE == 2 ? SM.item : SM.item * stride;
         const int32_t n = M.n;
+        const long long clen = MODE == 2 ? (long long)M.chunk : (long long)P.chunk;
         const long long local = item - M.item_base;
         const int dir = (int)(local & 1);
-        const long long nchunks = ((long long)n + P.chunk - 1) / P.chunk;
+        const long long nchunks = ((long long)n + clen - 1) / clen;
         const long long chunk = nchunks - 1 - (local >> 1);  // largest sources first
-        const int32_t s_first = (int32_t)(chunk * P.chunk);
-        const int32_t s_end = (int32_t)min((long long)n, (chunk + 1) * P.chunk);
+        const int32_t s_first = (int32_t)(chunk * clen);
+        const int32_t s_end = SM.skip ? s_first : (int32_t)min((long long)n, (chunk + 1) * clen);
         const long long words = bitmap_words_for(n);
         const long long nwords = ((long long)n + 31) >> 5;
+        if constexpr (MODE == 2) bm = words <= P.serve.smem_words ? sbm : gbm;
 
         Src S;
         S.n = n;
@@ -479,7 +679,7 @@ __global__ void __launch_bounds__(BLOCK, 1024 / BLOCK) traverse_kernel(TraverseL
                         SM.reached[(level + 1) % 3] = 0u;
                     }
                     S.reached = &SM.reached[level % 3];
-                    td_level<BLOCK>(S, q, qcap, lb, le, &SM.cnt[level % 3], P.status, P.heavy_len,
+                    td_level<BLOCK, CG>(S, q, qcap, lb, le, &SM.cnt[level % 3], P.status, P.heavy_len,
                                     raw, orig, trav);
                     __syncthreads();
                     const int nxt = SM.cnt[level % 3];
@@ -512,7 +712,7 @@ __global__ void __launch_bounds__(BLOCK, 1024 / BLOCK) traverse_kernel(TraverseL
                         SM.reached[(level + 1) % 3] = 0u;
                     }
                     S.reached = &SM.reached[level % 3];
-                    bu_sweep<BLOCK>(S, false, q, qcap, le, &SM.cnt[level % 3], P.status, trav);
+                    bu_sweep<BLOCK, CG>(S, false, q, qcap, le, &SM.cnt[level % 3], P.status, trav);
                     __syncthreads();
                     const int found = SM.cnt[level % 3];
                     level++;
@@ -540,7 +740,7 @@ __global__ void __launch_bounds__(BLOCK, 1024 / BLOCK) traverse_kernel(TraverseL
                 }
             }
             if (used_bu) {
-                bu_sweep<BLOCK>(S, true, q, qcap, le, nullptr, P.status, trav);
+                bu_sweep<BLOCK, CG>(S, true, q, qcap, le, nullptr, P.status, trav);
                 __syncthreads();
             }
 
@@ -607,13 +807,13 @@ __global__ void __launch_bounds__(BLOCK, 1024 / BLOCK) traverse_kernel(TraverseL
                 c_v += __popc(xl);
                 if (dir == 0 && xl) {
                     if (xl == ~0u) {
-                        c_e += (unsigned long long)__ldg(M.wdeg + w);
+                        c_e += (unsigned long long)ld_i32<CG>(M.wdeg + w);
                     } else {
                         uint32_t t = xl;
                         while (t) {
                             const int bp = __ffs(t) - 1;
                             t &= t - 1;
-                            c_e += (unsigned long long)row_degree(M.rowptr, (int)(base + bp));
+                            c_e += (unsigned long long)row_degree<CG>(M.rowptr, (int)(base + bp));
                         }
                     }
                 }
@@ -657,18 +857,9 @@ __global__ void __launch_bounds__(BLOCK, 1024 / BLOCK) traverse_kernel(TraverseL
                     M.nnz_lc[src] = (int32_t)gt;
                     if (digests) M.dig_lc[src] = r[5];
                 }
-                if (acc_mat != mi) {
-                    if (acc_mat >= 0) {
-                        unsigned long long* c = P.mats[acc_mat].counters;
-                        atomicAdd(&c[CNT_FILLS], acc[0]);
-                        atomicAdd(&c[CNT_EDGES_ALG], acc[1]);
-                        atomicAdd(&c[CNT_VERTS_ALG], acc[2]);
-                        atomicAdd(&c[CNT_EDGES_TRAV], acc[3]);
-                        atomicAdd(&c[CNT_NNZ_U], acc[4]);
-                        atomicAdd(&c[CNT_NNZ_L], acc[5]);
-                    }
+                if (MODE != 2 && acc_mat != mi) {
+                    if (acc_mat >= 0) flush_counters(P.mats[acc_mat].counters, acc);
                     acc_mat = mi;
-                    for (int j = 0; j < 6; j++) acc[j] = 0;
                 }
                 acc[0] += gt - og;
                 acc[3] += r[6];
@@ -682,38 +873,54 @@ __global__ void __launch_bounds__(BLOCK, 1024 / BLOCK) traverse_kernel(TraverseL
             }
             __syncthreads();
         }
+        if constexpr (MODE == 2) {
+            // publish this item's results, then count it; the CTA that
+            // finishes the request's last item tells the host
+            __threadfence();
+            __syncthreads();
+            if (threadIdx.x == 0) {
+                flush_counters(M.counters, acc);
+                __threadfence();
+                const unsigned long long d = atomicAdd(P.serve.items_done + M.slot, 1ull) + 1ull;
+                if (d == (unsigned long long)M.n_items) {
+                    __threadfence_system();
+                    *reinterpret_cast<volatile unsigned long long*>(P.serve.done_flags + M.slot) =
+                        M.seq;
+                }
+            }
+        }
     }
-    if (threadIdx.x == 0 && acc_mat >= 0) {
-        unsigned long long* c = P.mats[acc_mat].counters;
-        atomicAdd(&c[CNT_FILLS], acc[0]);
-        atomicAdd(&c[CNT_EDGES_ALG], acc[1]);
-        atomicAdd(&c[CNT_VERTS_ALG], acc[2]);
-        atomicAdd(&c[CNT_EDGES_TRAV], acc[3]);
-        atomicAdd(&c[CNT_NNZ_U], acc[4]);
-        atomicAdd(&c[CNT_NNZ_L], acc[5]);
+    if (MODE != 2 && threadIdx.x == 0 && acc_mat >= 0) flush_counters(P.mats[acc_mat].counters, acc);
+    if constexpr (MODE == 2) {
+        __syncthreads();  // the workspace is no longer in use
+        if (threadIdx.x == 0) {
+            __threadfence();
+            atomicSub(P.serve.alive, 1);
+            atomicAnd(P.serve.cta_slots + (SM.cta >> 5), ~(1u << (SM.cta & 31)));
+        }
     }
 }
 
-template <int BLOCK, bool SMEM_BM>
+template <int BLOCK, int MODE>
 static cudaError_t launch_one(const TraverseLaunch& L, int grid, size_t smem, cudaStream_t st) {
-    auto k = traverse_kernel<BLOCK, SMEM_BM>;
+    auto k = traverse_kernel<BLOCK, MODE>;
     cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)(SMEM_BM ? smem : 0));
+                                         (int)(MODE == 0 ? 0 : smem));
     if (e != cudaSuccess) return e;
-    k<<<grid, BLOCK, SMEM_BM ? smem : 0, st>>>(L);
+    k<<<grid, BLOCK, MODE == 0 ? 0 : smem, st>>>(L);
     return cudaGetLastError();
 }
 
-template <int BLOCK, bool SMEM_BM>
+template <int BLOCK, int MODE>
 static int occ_one(size_t smem) {
-    auto k = traverse_kernel<BLOCK, SMEM_BM>;
+    auto k = traverse_kernel<BLOCK, MODE>;
     if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)(SMEM_BM ? smem : 0)) != cudaSuccess) {
+                             (int)(MODE == 0 ? 0 : smem)) != cudaSuccess) {
         cudaGetLastError();
         return 0;
     }
     int blocks = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, k, BLOCK, SMEM_BM ? smem : 0) !=
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, k, BLOCK, MODE == 0 ? 0 : smem) !=
         cudaSuccess) {
         cudaGetLastError();
         return 0;
@@ -730,7 +937,7 @@ int traverse_block_sizes(int* sizes, int max_sizes) {
 
 int traverse_occupancy(int block, bool smem_bitmap, size_t smem) {
 #define OCC_CASE(B) \
-    case B: return smem_bitmap ? occ_one<B, true>(smem) : occ_one<B, false>(smem);
+    case B: return smem_bitmap ? occ_one<B, 1>(smem) : occ_one<B, 0>(smem);
     switch (block) {
         OCC_CASE(128)
         OCC_CASE(256)
@@ -744,8 +951,8 @@ int traverse_occupancy(int block, bool smem_bitmap, size_t smem) {
 cudaError_t launch_traverse(const TraverseLaunch& L, int block, int grid, bool smem_bitmap,
                             size_t smem, cudaStream_t st) {
 #define LAUNCH_CASE(B) \
-    case B: return smem_bitmap ? launch_one<B, true>(L, grid, smem, st) \
-                               : launch_one<B, false>(L, grid, smem, st);
+    case B: return smem_bitmap ? launch_one<B, 1>(L, grid, smem, st) \
+                               : launch_one<B, 0>(L, grid, smem, st);
     switch (block) {
         LAUNCH_CASE(128)
         LAUNCH_CASE(256)
@@ -754,6 +961,25 @@ cudaError_t launch_traverse(const TraverseLaunch& L, int block, int grid, bool s
         default: return cudaErrorInvalidValue;
     }
 #undef LAUNCH_CASE
+}
+
+int serve_occupancy(int block, size_t smem) {
+    switch (block) {
+        case 256: return occ_one<256, 2>(smem);
+        case 512: return occ_one<512, 2>(smem);
+        case 1024: return occ_one<1024, 2>(smem);
+        default: return 0;
+    }
+}
+
+cudaError_t launch_serve(const TraverseLaunch& L, int block, int grid, size_t smem,
+                         cudaStream_t st) {
+    switch (block) {
+        case 256: return launch_one<256, 2>(L, grid, smem, st);
+        case 512: return launch_one<512, 2>(L, grid, smem, st);
+        case 1024: return launch_one<1024, 2>(L, grid, smem, st);
+        default: return cudaErrorInvalidValue;
+    }
 }
 
 // ---- ingest: padded CSR of A and of A^T --------------------------------------
@@ -912,6 +1138,8 @@ cudaError_t launch_canonicalize(int32_t n, long long nnz_in, const int32_t* beg,
 // stays the first row.  Segments (runs between forced starts) hold <= 128
 // rows, so one warp handles one segment: 4 rows per lane, a warp max-scan
 // finds each row's start f, and the L-mask of column f answers L(r,f).
+// Inputs are read through L2: in serving they come from a traversal kernel
+// that is still running when this one starts.
 // One segment (<= 128 rows between forced starts) of one matrix, one warp.
 // Returns this lane's count of supernode starts and splits.
 __device__ __forceinline__ unsigned long long supernode_segment(
@@ -934,7 +1162,7 @@ __device__ __forceinline__ unsigned long long supernode_segment(
         const long long r = start + 4 * lane + j;
         head[j] = 0;
         if (r < stop) {
-            head[j] = (r == start) || (nzu[r - 1] - nzu[r] != 1);
+            head[j] = (r == start) || (__ldcg(nzu + r - 1) - __ldcg(nzu + r) != 1);
             if (head[j]) last = r;
         }
     }
@@ -958,7 +1186,7 @@ __device__ __forceinline__ unsigned long long supernode_segment(
             count++;
         } else {
             const long long bit = r - f - 1;  // 0..126
-            const uint32_t wv = lmask[4 * f + (bit >> 5)];
+            const uint32_t wv = __ldcg(lmask + 4 * f + (bit >> 5));
             const bool in_l = (wv >> (bit & 31)) & 1u;
             fl = in_l ? 0 : 2;
             if (!in_l) count++;

@@ -193,6 +193,71 @@ int gsofa_result_pattern_u(const gsofa_result* res, int64_t* ptr, int32_t* cols,
 int gsofa_result_pattern_l(const gsofa_result* res, int64_t* ptr, int32_t* rows, int64_t cap);
 int gsofa_result_destroy(gsofa_result* res);
 
+/* ---- serving: a request loop with continuous batching ------------------------ */
+/* No counterpart in the reference, which factors one matrix per run.  A server
+ * owns a host thread, three streams and a persistent traversal kernel that
+ * stays on the device while published work is waiting.  Each submitted matrix is a
+ * request; the loop admits requests in arrival order as slots and memory free
+ * up (its workspace footprint -- the padded CSR of A and A^T and its result
+ * arrays -- must fit the budget next to the requests already admitted),
+ * uploads and builds the matrix on a side stream, then publishes its work
+ * items to the running kernel.  The kernel's CTAs take items of every admitted
+ * request as they free up, so requests that arrive while others run share the
+ * device.  When a request's last item is done the loop runs its supernode
+ * detection and hands out a result identical to gsofa_factor_symbolic's
+ * (gsofa_result_* getters; the caller destroys it).
+ *
+ * opts: max_supernode_size and flags (GSOFA_SUPERNODES, GSOFA_DIGESTS,
+ * GSOFA_L_ROW_STATS; GSOFA_PATTERN is not served), threads_per_source (256,
+ * 512 or 1024; 0 = chosen from max_n), sources_in_flight (CTA cap),
+ * chunk_sources (0 = per request), cached_closures, heavy_row.  max_n is the
+ * largest order served (it sizes the per-CTA queues, closure rings and global
+ * bitmaps); budget_bytes bounds all device memory the server holds
+ * (0 = 40 GB). */
+typedef struct gsofa_server gsofa_server;
+int gsofa_server_create(gsofa_ctx* ctx, const gsofa_opts* opts, int32_t max_n,
+                        size_t budget_bytes, gsofa_server** out);
+/* Queues a request and returns at once with its ticket.  The arrays are read
+ * when the request is admitted: they must stay valid and unchanged until the
+ * ticket completes.  GSOFA_ERR_UNSUPPORTED if n > max_n, GSOFA_ERR_OOM_BUDGET
+ * if the request alone exceeds the budget, GSOFA_ERR_ARG after destroy began. */
+int gsofa_server_submit(gsofa_server* srv, int32_t n, int64_t nnz, const int32_t* row_begin,
+                        const int32_t* row_end, const int32_t* col, uint64_t* ticket);
+/* GSOFA_OK and *res once the ticket is complete (the result is handed out
+ * once; later calls return GSOFA_ERR_ARG), GSOFA_ERR_BUSY while it is queued
+ * or running, or the request's own error (malformed CSR: GSOFA_ERR_ARG). */
+int gsofa_server_poll(gsofa_server* srv, uint64_t ticket, gsofa_result** res);
+/* As poll, blocking up to timeout_ms (< 0: no limit); GSOFA_ERR_TIMEOUT when
+ * the time runs out first. */
+int gsofa_server_wait(gsofa_server* srv, uint64_t ticket, double timeout_ms, gsofa_result** res);
+typedef struct gsofa_ticket_info {
+    double t_submit_ms;   /* host clock, ms since the server was created      */
+    double t_admit_ms;    /* memory reserved, upload queued                   */
+    double t_publish_ms;  /* built on the device, work items claimable         */
+    double t_done_ms;     /* result complete (supernodes and totals read back) */
+    uint64_t footprint_bytes;
+    int32_t status;       /* GSOFA_OK, GSOFA_ERR_BUSY (not finished), or the error */
+    int32_t n;
+} gsofa_ticket_info;
+int gsofa_server_ticket_info(gsofa_server* srv, uint64_t ticket, gsofa_ticket_info* info);
+typedef struct gsofa_server_stats {
+    uint64_t submitted, completed, failed;
+    uint64_t kernel_launches;   /* persistent kernel (re)launches          */
+    uint64_t items_published;
+    uint64_t bytes_in_use;      /* workspace + admitted requests            */
+    uint64_t peak_bytes;
+    uint64_t fixed_bytes;       /* per-CTA queues, rings, bitmaps, tables   */
+    int32_t grid, block;        /* the kernel's CTAs and threads per CTA     */
+    int32_t max_in_flight;      /* most requests admitted at once           */
+    int32_t reserved;
+} gsofa_server_stats;
+int gsofa_server_get_stats(gsofa_server* srv, gsofa_server_stats* out);
+/* Finishes every queued request, stops the kernel and frees the server.
+ * Results already handed out stay valid; unclaimed ones are destroyed. */
+int gsofa_server_destroy(gsofa_server* srv);
+/* Message of the server's last internal error ("" if none). */
+const char* gsofa_server_last_error(const gsofa_server* srv);
+
 /* ---- factorization without device allocation --------------------------------- */
 /* No counterpart in the reference: an addition for callers that cannot call
  * cudaMalloc at factorization time (a host framework that owns all device

@@ -51,6 +51,22 @@ def test_no_gpu_is_an_error_code_not_a_crash():
     assert L.gsofa_symbfact_min_id(3, argv, 0, None, None, None, None) == _lib.ERR_ARG
 
 
+def test_server_calls_reject_null_handles():
+    """The serving entry points check their handles before touching a device."""
+    from gsofatpds_b200 import _lib
+    L = _lib.load()
+    h = ctypes.c_void_p()
+    t = ctypes.c_uint64()
+    assert L.gsofa_server_create(None, None, 1000, 0, ctypes.byref(h)) == _lib.ERR_ARG
+    assert L.gsofa_server_submit(None, 10, 10, None, None, None, ctypes.byref(t)) == _lib.ERR_ARG
+    assert L.gsofa_server_poll(None, 1, None) == _lib.ERR_ARG
+    assert L.gsofa_server_wait(None, 1, 0.0, None) == _lib.ERR_ARG
+    assert L.gsofa_server_ticket_info(None, 1, None) == _lib.ERR_ARG
+    assert L.gsofa_server_get_stats(None, None) == _lib.ERR_ARG
+    assert L.gsofa_server_destroy(None) == _lib.ERR_ARG
+    assert L.gsofa_server_last_error(None) == b"null server"
+
+
 def test_cli_usage_without_arguments():
     from gsofatpds_b200 import _lib
     out = subprocess.run([_lib.CLI_PATH], capture_output=True, text=True, timeout=60)
