@@ -261,6 +261,8 @@ MatDesc make_desc(const gsofa_matrix* m, const gsofa_result* r, long long base) 
     d.trowptr = m->trowptr;
     d.tcol = m->tcol;
     d.wdeg = m->wdeg;
+    d.dplanes = m->dplanes;
+    d.nplanes = m->nplanes;
     d.nnz_u = r->nnz_u;
     d.nz_row_u = r->nz_row_u;
     d.dig_u = r->dig_u;
@@ -487,6 +489,8 @@ bool gsofa::matrix_view(const void* mat, MatrixView* out) {
     out->trowptr = m->trowptr;
     out->tcol = m->tcol;
     out->wdeg = m->wdeg;
+    out->dplanes = m->dplanes;
+    out->nplanes = m->nplanes;
     return true;
 }
 
@@ -495,7 +499,7 @@ void gsofa::host::ingest_bytes(int32_t n, int64_t nnz, size_t* kept, size_t* sta
     const size_t N1 = (size_t)n + 1;
     const size_t PT = (size_t)std::max<int64_t>(nnz + 3ll * n, 4);
     const size_t NW = (size_t)(((int64_t)n + 31) >> 5) + 1;
-    *kept = align256(4 * N1) * 2 + align256(4 * PT) * 2 + align256(4 * NW);
+    *kept = align256(4 * N1) * 2 + align256(4 * PT) * 2 + align256(4 * NW) * 32;
     const size_t Nin = (size_t)std::max<int64_t>(nnz, 1);
     *staging = align256(4 * N1) + align256(4 * Nin) + align256(4 * N1) * 3 +
                align256(canonicalize_scan_bytes(n)) + 256;
@@ -512,7 +516,7 @@ int gsofa::host::ingest_csr(gsofa_ctx* ctx, cudaStream_t stream, int32_t* dstatu
     // host: padded row pointers of A.  Row v gets a multiple of 4 slots; the
     // number of padding slots of row v sits in the low 2 bits of rp[v+1].
     std::vector<int32_t> rp((size_t)n + 1);
-    int64_t acc = 0, real = 0;
+    int64_t acc = 0, real = 0, maxd = 0;
     rp[0] = 0;
     for (int32_t v = 0; v < n; v++) {
         const int64_t b = row_begin[v], e = row_end[v];
@@ -521,6 +525,7 @@ int gsofa::host::ingest_csr(gsofa_ctx* ctx, cudaStream_t stream, int32_t* dstatu
                            (long long)b, (long long)e, (long long)nnz);
         const int64_t d = e - b, pd = (d + 3) & ~(int64_t)3;
         real += d;
+        if (d > maxd) maxd = d;
         acc += pd;
         if (acc > INT32_MAX - 4 || real + 3ll * n > INT32_MAX - 4)
             return set_err(ctx, GSOFA_ERR_UNSUPPORTED, "padded nnz above 2^31");
@@ -537,7 +542,11 @@ int gsofa::host::ingest_csr(gsofa_ctx* ctx, cudaStream_t stream, int32_t* dstatu
     const size_t PA = (size_t)std::max<int64_t>(padded, 4);
     const size_t PT = (size_t)std::max<int64_t>(real + 3ll * n, 4);  // bound for A^T
     const size_t NW = (size_t)(((int64_t)n + 31) >> 5) + 1;
-    size_t total = align256(4 * N1) * 2 + align256(4 * PA) + align256(4 * PT) + align256(4 * NW);
+    int nplanes = 0;
+    while (nplanes < 32 && (maxd >> nplanes) != 0) nplanes++;
+    m->nplanes = nplanes;
+    size_t total = align256(4 * N1) * 2 + align256(4 * PA) + align256(4 * PT) + align256(4 * NW) +
+                   align256(4 * NW * (size_t)std::max(nplanes, 1));
     void* blk = nullptr;
     int rc = dev_alloc_on(ctx, total, &blk, stream);
     if (rc) { delete m; return rc; }
@@ -549,6 +558,8 @@ int gsofa::host::ingest_csr(gsofa_ctx* ctx, cudaStream_t stream, int32_t* dstatu
     m->tcol = reinterpret_cast<int32_t*>(b + 2 * align256(4 * N1) + align256(4 * PA));
     m->wdeg = reinterpret_cast<int32_t*>(b + 2 * align256(4 * N1) + align256(4 * PA) +
                                          align256(4 * PT));
+    m->dplanes = reinterpret_cast<uint32_t*>(b + 2 * align256(4 * N1) + align256(4 * PA) +
+                                             align256(4 * PT) + align256(4 * NW));
 
     // staging: raw input (beg, col_in) and the transpose's counters
     const size_t Nin = (size_t)std::max<int64_t>(nnz, 1);
@@ -593,7 +604,8 @@ int gsofa::host::ingest_csr(gsofa_ctx* ctx, cudaStream_t stream, int32_t* dstatu
     CKL(cudaMemsetAsync(tcount, 0, 4 * N1, stream));
     CKL(cudaMemsetAsync(tfill, 0, 4 * N1, stream));
     CKL(launch_canonicalize(n, nnz, dbeg, dcol_in, m->rowptr, m->col, tcount, tpad, m->trowptr,
-                            m->tcol, tfill, m->wdeg, scan_tmp, scan_bytes, dstatus, stream));
+                            m->tcol, tfill, m->wdeg, m->dplanes, m->nplanes, scan_tmp,
+                            scan_bytes, dstatus, stream));
 #undef CKL
     dev_free_on(ctx, sblk, stage, stream);  // stream-ordered: after the build
     *out = m;

@@ -51,6 +51,8 @@ struct gsofa_matrix {
     int32_t* trowptr = nullptr;
     int32_t* tcol = nullptr;
     int32_t* wdeg = nullptr;
+    uint32_t* dplanes = nullptr;
+    int32_t nplanes = 0;
     size_t bytes = 0;
 };
 

@@ -34,6 +34,9 @@ struct MatDesc {
     const int32_t* trowptr;     // n+1 (A^T)
     const int32_t* tcol;
     const int32_t* wdeg;        // ceil(n/32): sum of A's row lengths per 32-vertex word
+    const uint32_t* dplanes;    // nplanes * ceil(n/32): degree bit-planes of A's rows
+    int32_t nplanes;            // bits of A's largest row length
+    int32_t pad0;
     int32_t* nnz_u;             // n: |U row|
     int32_t* nz_row_u;          // n: reference nz_row_U counter
     uint64_t* dig_u;            // n (or null)
@@ -131,8 +134,9 @@ cudaError_t launch_serve(const TraverseLaunch& L, int block, int grid, size_t sm
 cudaError_t launch_canonicalize(int32_t n, long long nnz_in, const int32_t* beg,
                                 const int32_t* col_in, const int32_t* rp, int32_t* col_out,
                                 int32_t* tcount, int32_t* tpad, int32_t* trp, int32_t* tcol,
-                                int32_t* tfill, int32_t* wdeg, void* scan_tmp,
-                                size_t scan_tmp_bytes, int32_t* status, cudaStream_t stream);
+                                int32_t* tfill, int32_t* wdeg, uint32_t* dplanes, int nplanes,
+                                void* scan_tmp, size_t scan_tmp_bytes, int32_t* status,
+                                cudaStream_t stream);
 size_t canonicalize_scan_bytes(int32_t n);
 cudaError_t launch_supernodes(int32_t n, int32_t mss, const int32_t* nz_row_u,
                               const uint32_t* lmask, int8_t* flags,
@@ -157,6 +161,8 @@ struct MatrixView {
     const int32_t* trowptr;
     const int32_t* tcol;
     const int32_t* wdeg;
+    const uint32_t* dplanes;
+    int32_t nplanes;
 };
 bool matrix_view(const void* mat, MatrixView* out);
 

@@ -101,6 +101,9 @@ struct TraverseSmem {
     int mi;               // matrix of the current item
     int skip;             // the current item's matrix failed ingest: count it only
     int cta;              // workspace slot (serving) or block index
+    int wlo, whi;         // bitmap words holding the current source's set bits
+    int ring_lo[32];      // per ring slot: the words its closure occupies
+    int ring_hi[32];
 };
 
 // Bitmap words of a matrix of order n: n bits plus zero padding read by the
@@ -121,6 +124,8 @@ struct Src {
     // current chunk: source t lives in slot t & (ring-1).  Sources in
     // [cache_lo, src) are cached; merged_mask has the slots already merged.
     const uint32_t* ring_base;
+    const int* ring_lo;               // per slot: first and last word of its closure
+    const int* ring_hi;               // (words outside hold stale data from older closures)
     long long words;                  // ring slot stride (the launch's widest bitmap)
     long long mwords;                 // this matrix's bitmap words (what a merge ORs)
     int ring;
@@ -143,9 +148,11 @@ __device__ __forceinline__ int32_t slot_source(const Src& S, int j) {
 // expanded.)  Only an optimisation: a false "no" costs one needless expansion.
 __device__ __forceinline__ bool covered(const Src& S, int top, int32_t v) {
     if (top < 0 || v > slot_source(S, top)) return false;
+    const int w = v >> 5;
+    if (w < S.ring_lo[top] || w > S.ring_hi[top]) return false;  // no set bit there
     // plain load: the ring is written by this kernel
     const uint32_t* y = S.ring_base + (long long)top * S.words;
-    return (y[v >> 5] >> (v & 31)) & 1u;
+    return (y[w] >> (v & 31)) & 1u;
 }
 
 // Slot of the largest source in a merged mask, or -1.
@@ -159,12 +166,17 @@ __device__ __forceinline__ int top_slot(const Src& S, uint32_t mask) {
 // to queue.  w == src (also the sentinel of idle lanes and the padding of the
 // source's row) is a no-op.  raw / orig count the source row's entries > src
 // (with multiplicity / distinct) for the reference's nz_row_U counter.
-__device__ __forceinline__ bool td_edge(const Src& S, int v, int w, uint32_t& raw, uint32_t& orig) {
+__device__ __forceinline__ bool td_edge(const Src& S, int v, int w, uint32_t& raw, uint32_t& orig,
+                                        int& wl, int& wh) {
     if (w == S.src) return false;
     const uint32_t bit = 1u << (w & 31);
     uint32_t* word = S.bm + (w >> 5);
     bool fresh = false;
     if (!(ld_vol(word) & bit)) fresh = !(atomicOr(word, bit) & bit);
+    if (fresh) {  // the set bits' word range (census and ring copy)
+        wl = min(wl, w >> 5);
+        wh = max(wh, w >> 5);
+    }
     if (w > S.src) {
         if (v == S.src) {
             raw++;
@@ -207,12 +219,12 @@ __device__ __forceinline__ void push4(int32_t* q, long long qcap, long long le, 
 }
 
 __device__ __forceinline__ unsigned td_edge4(const Src& S, int v, const int4& e, uint32_t& raw,
-                                             uint32_t& orig) {
+                                             uint32_t& orig, int& wl, int& wh) {
     unsigned f = 0;
-    if (td_edge(S, v, e.x, raw, orig)) f |= 1u;
-    if (td_edge(S, v, e.y, raw, orig)) f |= 2u;
-    if (td_edge(S, v, e.z, raw, orig)) f |= 4u;
-    if (td_edge(S, v, e.w, raw, orig)) f |= 8u;
+    if (td_edge(S, v, e.x, raw, orig, wl, wh)) f |= 1u;
+    if (td_edge(S, v, e.y, raw, orig, wl, wh)) f |= 2u;
+    if (td_edge(S, v, e.z, raw, orig, wl, wh)) f |= 4u;
+    if (td_edge(S, v, e.w, raw, orig, wl, wh)) f |= 8u;
     return f;
 }
 
@@ -222,7 +234,8 @@ __device__ __forceinline__ unsigned td_edge4(const Src& S, int v, const int4& e,
 template <int BLOCK, bool CG>
 __device__ __forceinline__ void td_level(const Src& S, int32_t* q, long long qcap, long long lb,
                                          long long le, int* cnt, int32_t* status, int heavy_len,
-                                         uint32_t& raw, uint32_t& orig, uint32_t& trav) {
+                                         uint32_t& raw, uint32_t& orig, uint32_t& trav, int& wl,
+                                         int& wh) {
     constexpr int NW = BLOCK / 32;
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
@@ -257,7 +270,7 @@ __device__ __forceinline__ void td_level(const Src& S, int32_t* q, long long qca
             for (int k0 = 0; k0 < hl; k0 += 128) {
                 const int k = k0 + 4 * lane;
                 const int4 e = k < hl ? ld_row4<CG>(S.cl + hb + k) : idle;
-                const unsigned f = td_edge4(S, hv, e, raw, orig);
+                const unsigned f = td_edge4(S, hv, e, raw, orig, wl, wh);
                 push4(q, qcap, le, cnt, status, lane, e, f);
             }
         }
@@ -267,7 +280,7 @@ __device__ __forceinline__ void td_level(const Src& S, int32_t* q, long long qca
         const int maxit = __reduce_max_sync(FULL_MASK, its);
         for (int it = 0; it < maxit; it++) {
             const int4 e = it < its ? ld_row4<CG>(S.cl + s0 + 4 * it) : idle;
-            const unsigned f = td_edge4(S, v, e, raw, orig);
+            const unsigned f = td_edge4(S, v, e, raw, orig, wl, wh);
             push4(q, qcap, le, cnt, status, lane, e, f);
         }
     }
@@ -338,7 +351,8 @@ template <int BLOCK>
 __device__ __forceinline__ uint32_t merge_reached(const Src& S, uint32_t reached, uint32_t* bm,
                                                   int32_t* q, long long at, long long qcap,
                                                   int* pushed, uint32_t* pending_out,
-                                                  int32_t* status, bool& did_merge) {
+                                                  int32_t* status, bool& did_merge, int& wl,
+                                                  int& wh) {
     // The decision uses only values every thread holds identically: the
     // level's reached mask (stable until two levels later), the pending mask
     // and the ring, never the live bitmap.
@@ -372,12 +386,34 @@ __device__ __forceinline__ uint32_t merge_reached(const Src& S, uint32_t reached
         b1 = ld_vol(bm + w1);
         __syncthreads();
     }
-    for (long long i = threadIdx.x; i < S.mwords; i += BLOCK) {
-        uint32_t x = bm[i];
-        for (uint32_t a = add; a; a &= a - 1)
-            x |= S.ring_base[(long long)(__ffs(a) - 1) * S.words + i];
-        bm[i] = x;
+    // OR the added closures over the words they occupy, four words per
+    // thread per pass so that their loads overlap
+    int mlo = INT_MAX, mhi = -1;
+    for (uint32_t a = add; a; a &= a - 1) {
+        const int sl = __ffs(a) - 1;
+        mlo = min(mlo, S.ring_lo[sl]);
+        mhi = max(mhi, S.ring_hi[sl]);
     }
+    for (long long i0 = (long long)mlo + threadIdx.x; i0 <= mhi; i0 += 4ll * BLOCK) {
+        uint32_t y[4] = {0u, 0u, 0u, 0u};
+        for (uint32_t a = add; a; a &= a - 1) {
+            const int sl = __ffs(a) - 1;
+            const int slo = S.ring_lo[sl], shi = S.ring_hi[sl];
+            const uint32_t* src = S.ring_base + (long long)sl * S.words;
+#pragma unroll
+            for (int j = 0; j < 4; j++) {
+                const long long i = i0 + (long long)j * BLOCK;
+                if (i >= slo && i <= shi) y[j] |= src[i];
+            }
+        }
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+            const long long i = i0 + (long long)j * BLOCK;
+            if (i <= mhi && y[j]) bm[i] |= y[j];
+        }
+    }
+    wl = min(wl, mlo);
+    wh = max(wh, mhi);
     if (!window) {
         if (threadIdx.x == 0) {
             *pushed = 0;
@@ -637,6 +673,8 @@ __global__ void __launch_bounds__(BLOCK, 1024 / BLOCK) traverse_kernel(TraverseL
         S.icl = dir ? M.col : M.tcol;
         S.bm = bm;
         S.ring_base = ring_base;
+        S.ring_lo = SM.ring_lo;
+        S.ring_hi = SM.ring_hi;
         S.words = P.bitmap_words;
         S.mwords = words;
         S.ring = P.ring;
@@ -658,8 +696,11 @@ __global__ void __launch_bounds__(BLOCK, 1024 / BLOCK) traverse_kernel(TraverseL
                 SM.cnt[0] = 0;
                 SM.reached[0] = 0u;
                 SM.abort_level = 0;
+                SM.wlo = SM.whi = src >> 5;
             }
             __syncthreads();
+            // this thread's share of the set bits' word range
+            int wl = src >> 5, wh = src >> 5;
 
             uint32_t raw = 0, orig = 0, trav = 0;
             long long lb = 0, le = 1;
@@ -680,7 +721,7 @@ __global__ void __launch_bounds__(BLOCK, 1024 / BLOCK) traverse_kernel(TraverseL
                     }
                     S.reached = &SM.reached[level % 3];
                     td_level<BLOCK, CG>(S, q, qcap, lb, le, &SM.cnt[level % 3], P.status, P.heavy_len,
-                                    raw, orig, trav);
+                                    raw, orig, trav, wl, wh);
                     __syncthreads();
                     const int nxt = SM.cnt[level % 3];
                     level++;
@@ -690,7 +731,7 @@ __global__ void __launch_bounds__(BLOCK, 1024 / BLOCK) traverse_kernel(TraverseL
                     const uint32_t mm =
                         S.cache_lo < src
                             ? merge_reached<BLOCK>(S, reached, bm, q, le + nxt, qcap, &SM.pushed,
-                                                   &SM.pending, P.status, did)
+                                                   &SM.pending, P.status, did, wl, wh)
                             : S.merged_mask;
                     if (mm != S.merged_mask) {
                         S.merged_mask = mm;
@@ -724,7 +765,7 @@ __global__ void __launch_bounds__(BLOCK, 1024 / BLOCK) traverse_kernel(TraverseL
                     const uint32_t mm =
                         S.cache_lo < src
                             ? merge_reached<BLOCK>(S, reached, bm, q, le, qcap, &SM.pushed,
-                                                   &SM.pending, P.status, did)
+                                                   &SM.pending, P.status, did, wl, wh)
                             : S.merged_mask;
                     if (mm != S.merged_mask) {
                         S.merged_mask = mm;
@@ -742,7 +783,18 @@ __global__ void __launch_bounds__(BLOCK, 1024 / BLOCK) traverse_kernel(TraverseL
             if (used_bu) {
                 bu_sweep<BLOCK, CG>(S, true, q, qcap, le, nullptr, P.status, trav);
                 __syncthreads();
+                wl = 0;  // sweeps set bits anywhere
+                wh = (int)nwords - 1;
             }
+            // the block's word range of set bits
+            wl = __reduce_min_sync(FULL_MASK, wl);
+            wh = __reduce_max_sync(FULL_MASK, wh);
+            if (lane == 0) {
+                atomicMin(&SM.wlo, wl);
+                atomicMax(&SM.whi, wh);
+            }
+            __syncthreads();
+            const long long wlo = SM.wlo, whi = SM.whi;
 
             if (dir == 1 && !P.pattern_pass && threadIdx.x < 4) {
                 // 128-bit mask of rows f+1 .. f+128 in L column f (supernode test)
@@ -789,7 +841,12 @@ __global__ void __launch_bounds__(BLOCK, 1024 / BLOCK) traverse_kernel(TraverseL
             unsigned long long c_gt = 0, c_v = 0, c_e = 0, c_dig = 0;
             const bool keep = P.merge && src + 1 < s_end;
             uint32_t* keep_slot = ring_base + (long long)(src & (P.ring - 1)) * P.bitmap_words;
-            for (long long w = threadIdx.x; w < words; w += BLOCK) {
+            if (keep && threadIdx.x == 0) {
+                SM.ring_lo[src & (P.ring - 1)] = (int)wlo;
+                SM.ring_hi[src & (P.ring - 1)] = (int)whi;
+            }
+            // every set bit lies in words [wlo, whi]: the rest of the bitmap is zero
+            for (long long w = wlo + threadIdx.x; w <= whi; w += BLOCK) {
                 const uint32_t x = bm[w];
                 bm[w] = 0u;
                 if (keep) keep_slot[w] = x;
@@ -808,13 +865,19 @@ __global__ void __launch_bounds__(BLOCK, 1024 / BLOCK) traverse_kernel(TraverseL
                 if (dir == 0 && xl) {
                     if (xl == ~0u) {
                         c_e += (unsigned long long)ld_i32<CG>(M.wdeg + w);
-                    } else {
+                    } else if (__popc(xl) <= 4 || M.dplanes == nullptr) {
                         uint32_t t = xl;
                         while (t) {
                             const int bp = __ffs(t) - 1;
                             t &= t - 1;
                             c_e += (unsigned long long)row_degree<CG>(M.rowptr, (int)(base + bp));
                         }
+                    } else {
+                        // degree sum from the bit-planes: a few coalesced loads
+                        const int32_t* pl = reinterpret_cast<const int32_t*>(M.dplanes) + w;
+                        for (int k = 0; k < M.nplanes; k++)
+                            c_e += (unsigned long long)__popc(xl & (uint32_t)ld_i32<CG>(pl + k * nwords))
+                                   << k;
                     }
                 }
                 c_gt += __popc(xh);
@@ -1063,9 +1126,13 @@ __global__ void transpose_scatter_kernel(int32_t n, const int32_t* __restrict__ 
     }
 }
 
-// wdeg[w] = total length of A's rows 32w .. 32w+31 (census of full words).
+// wdeg[w] = total length of A's rows 32w .. 32w+31 (census of full words),
+// and the degree bit-planes: bit j of planes[k * nw + w] is bit k of the
+// length of row 32w + j, so the degree sum over any set x of word w's
+// vertices is sum_k 2^k popc(x & planes[k * nw + w]).
 __global__ void word_degree_kernel(int32_t n, const int32_t* __restrict__ rp,
-                                   int32_t* __restrict__ wdeg) {
+                                   int32_t* __restrict__ wdeg, uint32_t* __restrict__ planes,
+                                   int nplanes) {
     const long long nw = ((long long)n + 31) >> 5;
     const int lane = threadIdx.x & 31;
     const long long gw = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -1076,9 +1143,14 @@ __global__ void word_degree_kernel(int32_t n, const int32_t* __restrict__ rp,
             const int r0 = rp[v], r1 = rp[v + 1];
             d = (r1 & ~3) - (r0 & ~3) - (r1 & 3);
         }
+        for (int k = 0; k < nplanes; k++) {
+            const unsigned b = __ballot_sync(FULL_MASK, (d >> k) & 1);
+            if (lane == 0) planes[(long long)k * nw + w] = b;
+        }
+        int sum = d;
 #pragma unroll
-        for (int o = 16; o > 0; o >>= 1) d += __shfl_xor_sync(FULL_MASK, d, o);
-        if (lane == 0) wdeg[w] = d;
+        for (int o = 16; o > 0; o >>= 1) sum += __shfl_xor_sync(FULL_MASK, sum, o);
+        if (lane == 0) wdeg[w] = sum;
     }
 }
 
@@ -1103,8 +1175,9 @@ size_t canonicalize_scan_bytes(int32_t n) {
 cudaError_t launch_canonicalize(int32_t n, long long nnz_in, const int32_t* beg,
                                 const int32_t* col_in, const int32_t* rp, int32_t* col_out,
                                 int32_t* tcount, int32_t* tpad, int32_t* trp, int32_t* tcol,
-                                int32_t* tfill, int32_t* wdeg, void* scan_tmp,
-                                size_t scan_tmp_bytes, int32_t* status, cudaStream_t st) {
+                                int32_t* tfill, int32_t* wdeg, uint32_t* dplanes, int nplanes,
+                                void* scan_tmp, size_t scan_tmp_bytes, int32_t* status,
+                                cudaStream_t st) {
     if (n <= 0) return cudaSuccess;
     const int threads = 256;
     long long grid_w = ((long long)n * 32 + threads - 1) / threads;
@@ -1125,7 +1198,7 @@ cudaError_t launch_canonicalize(int32_t n, long long nnz_in, const int32_t* beg,
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
     transpose_pad_kernel<<<gridt, threads, 0, st>>>(n, tcount, trp, tcol);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
-    word_degree_kernel<<<gridt, threads, 0, st>>>(n, rp, wdeg);
+    word_degree_kernel<<<gridt, threads, 0, st>>>(n, rp, wdeg, dplanes, nplanes);
     return cudaGetLastError();
 }
 

@@ -145,6 +145,8 @@ extern "C" int gsofa_factor_symbolic_noalloc(const gsofa_matrix* mat, const gsof
     d.trowptr = mv.trowptr;
     d.tcol = mv.tcol;
     d.wdeg = mv.wdeg;
+    d.dplanes = mv.dplanes;
+    d.nplanes = mv.nplanes;
     d.nnz_u = d_nnz_u_row;
     d.nz_row_u = d_nz_row_u;
     d.nnz_lc = d_nnz_l_col;
