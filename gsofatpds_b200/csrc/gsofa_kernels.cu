@@ -43,7 +43,9 @@ namespace gsofa {
 
 #define FULL_MASK 0xffffffffu
 
-// Column-set digest term: splitmix64 finaliser (Steele, Lea, Flood 2014).
+// Digest mixing: splitmix64 finaliser (Steele, Lea, Flood 2014).  A U-row
+// or L-column digest sums mix64((w << 32) | mask) over the set's non-zero
+// 32-id words w; an L-row digest (scattered) sums mix64(id) over its ids.
 __host__ __device__ __forceinline__ uint64_t mix64(uint64_t x) {
     x += 0x9E3779B97F4A7C15ull;
     x = (x ^ (x >> 30)) * 0xBF58476D1CE4E5B9ull;
@@ -94,6 +96,7 @@ struct TraverseSmem {
     unsigned long long red[BLOCK / 32][7];
     long long item;
     int cnt[3];
+    int grab[3];          // per level (rotating): 32-vertex chunks of the frontier taken
     int abort_level;  // set when a cached source is reached: stop, merge, redo
     int pushed;       // ids a merge appended to the queue
     unsigned pending; // cached sources a merge set (slots), for the next decision
@@ -233,14 +236,23 @@ __device__ __forceinline__ unsigned td_edge4(const Src& S, int v, const int4& e,
 // are skipped: their reach is already in the bitmap.
 template <int BLOCK, bool CG>
 __device__ __forceinline__ void td_level(const Src& S, int32_t* q, long long qcap, long long lb,
-                                         long long le, int* cnt, int32_t* status, int heavy_len,
-                                         uint32_t& raw, uint32_t& orig, uint32_t& trav, int& wl,
-                                         int& wh) {
+                                         long long le, int* cnt, int* grab, int32_t* status,
+                                         int heavy_len, uint32_t& raw, uint32_t& orig,
+                                         uint32_t& trav, int& wl, int& wh) {
     constexpr int NW = BLOCK / 32;
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
     const int4 idle = make_int4(S.src, S.src, S.src, S.src);
-    for (long long base = lb + warp * 32; base < le; base += NW * 32) {
+    (void)NW;
+    (void)warp;
+    // warps take 32-vertex chunks of the frontier as they free up: rows of
+    // very uneven length would leave statically assigned warps idle at the
+    // level's barrier
+    for (;;) {
+        int chunk = 0;
+        if (lane == 0) chunk = atomicAdd(grab, 1);
+        const long long base = lb + 32ll * __shfl_sync(FULL_MASK, chunk, 0);
+        if (base >= le) break;
         // stop when a cached source was reached; one value for the whole warp
         const int ab = __shfl_sync(FULL_MASK, *(volatile int*)S.abort_flag, 0);
         if (lb > 0 && ab) break;
@@ -278,10 +290,14 @@ __device__ __forceinline__ void td_level(const Src& S, int32_t* q, long long qca
         // short rows: one lane per vertex, 4 entries per int4 load
         const int its = plen >> 2;
         const int maxit = __reduce_max_sync(FULL_MASK, its);
+        // the next int4 of the row is loaded before this one is processed, so
+        // two loads of each lane's chain are in flight
+        int4 e = 0 < its ? ld_row4<CG>(S.cl + s0) : idle;
         for (int it = 0; it < maxit; it++) {
-            const int4 e = it < its ? ld_row4<CG>(S.cl + s0 + 4 * it) : idle;
+            const int4 nx = it + 1 < its ? ld_row4<CG>(S.cl + s0 + 4 * (it + 1)) : idle;
             const unsigned f = td_edge4(S, v, e, raw, orig, wl, wh);
             push4(q, qcap, le, cnt, status, lane, e, f);
+            e = nx;
         }
     }
 }
@@ -694,6 +710,7 @@ __global__ void __launch_bounds__(BLOCK, 1024 / BLOCK) traverse_kernel(TraverseL
                 bm[src >> 5] |= 1u << (src & 31);
                 q[0] = src;
                 SM.cnt[0] = 0;
+                SM.grab[0] = 0;
                 SM.reached[0] = 0u;
                 SM.abort_level = 0;
                 SM.wlo = SM.whi = src >> 5;
@@ -717,11 +734,12 @@ __global__ void __launch_bounds__(BLOCK, 1024 / BLOCK) traverse_kernel(TraverseL
                     }
                     if (threadIdx.x == 0) {
                         SM.cnt[(level + 1) % 3] = 0;
+                        SM.grab[(level + 1) % 3] = 0;
                         SM.reached[(level + 1) % 3] = 0u;
                     }
                     S.reached = &SM.reached[level % 3];
-                    td_level<BLOCK, CG>(S, q, qcap, lb, le, &SM.cnt[level % 3], P.status, P.heavy_len,
-                                    raw, orig, trav, wl, wh);
+                    td_level<BLOCK, CG>(S, q, qcap, lb, le, &SM.cnt[level % 3], &SM.grab[level % 3],
+                                        P.status, P.heavy_len, raw, orig, trav, wl, wh);
                     __syncthreads();
                     const int nxt = SM.cnt[level % 3];
                     level++;
@@ -750,6 +768,7 @@ __global__ void __launch_bounds__(BLOCK, 1024 / BLOCK) traverse_kernel(TraverseL
                     const long long unseen = (long long)src - (le - 1);
                     if (threadIdx.x == 0) {
                         SM.cnt[(level + 1) % 3] = 0;
+                        SM.grab[(level + 1) % 3] = 0;
                         SM.reached[(level + 1) % 3] = 0u;
                     }
                     S.reached = &SM.reached[level % 3];
@@ -881,18 +900,17 @@ __global__ void __launch_bounds__(BLOCK, 1024 / BLOCK) traverse_kernel(TraverseL
                     }
                 }
                 c_gt += __popc(xh);
-                if ((digests || scatter) && xh) {
+                // U-row / L-column digest: one term per non-zero word
+                if (digests && xh) c_dig += mix64(((uint64_t)w << 32) | xh);
+                if (scatter && xh) {
+                    const unsigned long long ds = mix64((uint64_t)src);
                     uint32_t t = xh;
                     while (t) {
                         const int bp = __ffs(t) - 1;
                         t &= t - 1;
                         const int wv = (int)(base + bp);
-                        if (digests) c_dig += mix64((uint64_t)wv);
-                        if (scatter) {
-                            atomicAdd(&M.nnz_lr[wv], 1);
-                            atomicAdd((unsigned long long*)&M.dig_lr[wv],
-                                      (unsigned long long)mix64((uint64_t)src));
-                        }
+                        atomicAdd(&M.nnz_lr[wv], 1);
+                        atomicAdd((unsigned long long*)&M.dig_lr[wv], ds);
                     }
                 }
             }

@@ -173,7 +173,10 @@ int gsofa_result_counts(const gsofa_result* res, gsofa_counts* out);
  *   nnz_l_row[v]  distinct strictly-lower entries of row v (needs GSOFA_L_ROW_STATS) */
 int gsofa_result_row_counts(const gsofa_result* res, int32_t* nnz_u_row, int32_t* nz_row_u,
                             int32_t* nnz_l_col, int32_t* nnz_l_row);
-/* Column-set digests: sum mod 2^64 of splitmix64(column id) over the set. */
+/* Column-set digests (mod 2^64 sums of the splitmix64 finaliser): for U rows
+ * and L columns, sum over the set's non-zero 32-id words w of
+ * splitmix64((w << 32) | mask_w) (bit j of mask_w: id 32w + j in the set);
+ * for L rows (GSOFA_L_ROW_STATS), sum of splitmix64(column id). */
 int gsofa_result_digests(const gsofa_result* res, uint64_t* dig_u_row, uint64_t* dig_l_col,
                          uint64_t* dig_l_row);
 /* Supernode partition: flags[v] (n bytes) = 1 row starts a supernode, 2 a

@@ -45,6 +45,8 @@ typedef struct {
     int32_t* pnext;    /* bucket pool: next index */
     int64_t pcap, plen;
     int32_t* tmp;      /* sort scratch for pattern output */
+    uint32_t* wmask;   /* (n+31)/32 word masks of the U column set, kept zero */
+    int32_t* wlist;    /* words with a non-zero mask */
 } or_ws;
 
 static int ws_init(or_ws* w, int32_t n) {
@@ -54,10 +56,14 @@ static int ws_init(or_ws* w, int32_t n) {
     w->bhead = (int32_t*)malloc(sizeof(int32_t) * (size_t)(n + 2));
     w->touched = (int32_t*)malloc(sizeof(int32_t) * (size_t)(n + 1));
     w->tmp = (int32_t*)malloc(sizeof(int32_t) * (size_t)(n + 1));
+    w->wmask = (uint32_t*)calloc((size_t)n / 32 + 2, sizeof(uint32_t));
+    w->wlist = (int32_t*)malloc(sizeof(int32_t) * ((size_t)n / 32 + 2));
     w->pcap = 1024;
     w->pv = (int32_t*)malloc(sizeof(int32_t) * (size_t)w->pcap);
     w->pnext = (int32_t*)malloc(sizeof(int32_t) * (size_t)w->pcap);
-    if (!w->lab || !w->done || !w->bhead || !w->touched || !w->tmp || !w->pv || !w->pnext) return -1;
+    if (!w->lab || !w->done || !w->bhead || !w->touched || !w->tmp || !w->pv || !w->pnext ||
+        !w->wmask || !w->wlist)
+        return -1;
     for (int64_t i = 0; i <= n; i++) w->lab[i] = OR_INF;
     for (int64_t i = 0; i < (int64_t)n + 2; i++) w->bhead[i] = -1;
     return 0;
@@ -65,7 +71,7 @@ static int ws_init(or_ws* w, int32_t n) {
 
 static void ws_free(or_ws* w) {
     free(w->lab); free(w->done); free(w->bhead); free(w->touched);
-    free(w->tmp); free(w->pv); free(w->pnext);
+    free(w->tmp); free(w->pv); free(w->pnext); free(w->wmask); free(w->wlist);
 }
 
 static int push(or_ws* w, int32_t v, uint32_t key) {
@@ -149,7 +155,7 @@ static int one_row(or_ws* w, int32_t n, const int32_t* beg, const int32_t* end,
         }
     }
     /* collect results from the final labels */
-    int64_t cL = 0, cU = 0;
+    int64_t cL = 0, cU = 0, nwl = 0;
     uint64_t dL = 0, dU = 0;
     uint32_t lb[4] = {0, 0, 0, 0};
     for (int64_t t = 0; t < w->ntouched; t++) {
@@ -164,8 +170,16 @@ static int one_row(or_ws* w, int32_t n, const int32_t* beg, const int32_t* end,
             }
         } else {
             cU++;
-            dU += or_mix64((uint64_t)v);
+            uint32_t* m = &w->wmask[v >> 5];
+            if (!*m) w->wlist[nwl++] = v >> 5;
+            *m |= 1u << (v & 31);
         }
+    }
+    /* U digest: one term per non-zero 32-column word (word index, mask) */
+    for (int64_t k = 0; k < nwl; k++) {
+        const int32_t wd = w->wlist[k];
+        dU += or_mix64(((uint64_t)(uint32_t)wd << 32) | w->wmask[wd]);
+        w->wmask[wd] = 0;
     }
     if (nnzL) nnzL[i] = (int32_t)cL;
     if (nnzU) nnzU[i] = (int32_t)cU;

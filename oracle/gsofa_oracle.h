@@ -25,9 +25,11 @@
 extern "C" {
 #endif
 
-/* Order-independent 64-bit digest term of one column id (splitmix64 finaliser,
- * Steele/Lea/Flood 2014).  A row digest is the sum (mod 2^64) of this term
- * over the row's column set. */
+/* splitmix64 finaliser (Steele/Lea/Flood 2014), the digest mixing function.
+ * A U-row digest is the sum (mod 2^64) of or_mix64((w << 32) | mask_w) over
+ * the non-zero 32-column words w of the row's column set (mask_w: bit j set
+ * iff column 32w + j is in the set); an L-row digest is the sum of
+ * or_mix64(column id) over the set. */
 uint64_t or_mix64(uint64_t x);
 
 /*
@@ -39,7 +41,8 @@ uint64_t or_mix64(uint64_t x);
  *                     rows[i] in L+U (originals + fills)
  *   nzU_ref[i]        the reference's nz_row_U counter (CSR entries > row with
  *                     multiplicity, plus fills > row)
- *   digL[i], digU[i]  digests of the L / U column sets
+ *   digL[i], digU[i]  digests of the L column set (per column) and of the U
+ *                     column set (per 32-column word), see or_mix64
  *   fills[i]          fill entries of the row (not in A, off-diagonal)
  *   e_alg[i], v_alg[i] edges inspected / vertices expanded by an ideal search
  *                     (vertices v < row reachable through vertices < row)

@@ -143,3 +143,25 @@ def test_transposed_reachability_equals_labels():
                 Lcol[m].append(s)
         for m in range(n):
             assert sorted(Lcol[m]) == list(rt["Ucols"][rt["Uptr"][m]:rt["Uptr"][m + 1]])
+
+
+@pytest.mark.parametrize("seed", range(4))
+def test_digest_definitions(seed):
+    """U-row digests sum splitmix64((w << 32) | mask) over the row's non-zero
+    32-column words; L-row digests sum splitmix64(column) over its columns."""
+    rng = np.random.default_rng(100 + seed)
+    n = int(rng.integers(40, 200))
+    pat = random_pattern(rng, n, rng.uniform(0.02, 0.1), diag=True)
+    beg, end, col = scrambled_csr(rng, pat)
+    r = O.rows(beg, end, col, pattern=True)
+    M = (1 << 64) - 1
+    for s in range(n):
+        U = r["Ucols"][r["Uptr"][s]:r["Uptr"][s + 1]]
+        words = {}
+        for c in U:
+            words[int(c) >> 5] = words.get(int(c) >> 5, 0) | (1 << (int(c) & 31))
+        du = sum(O.mix64((w << 32) | m) for w, m in words.items()) & M
+        assert du == int(r["digU"][s]), (seed, s)
+        L = r["Lcols"][r["Lptr"][s]:r["Lptr"][s + 1]]
+        dl = sum(O.mix64(int(c)) for c in L) & M
+        assert dl == int(r["digL"][s]), (seed, s)
