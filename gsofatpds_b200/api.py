@@ -108,7 +108,7 @@ class Context:
         o = self.opts(**kw)
         self._check(self._L.gsofa_autotune(self._h, mat.handle, ctypes.byref(o)), "autotune")
         return dict(threads_per_source=o.threads_per_source, chunk_sources=o.chunk_sources,
-                    cached_closures=o.cached_closures)
+                    cached_closures=o.cached_closures, heavy_row=o.heavy_row)
 
     def factor(self, mat, **kw):
         o = self.opts(**kw)

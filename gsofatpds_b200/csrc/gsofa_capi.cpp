@@ -859,6 +859,7 @@ int gsofa_autotune(gsofa_ctx* ctx, const gsofa_matrix* mat, gsofa_opts* opts) {
         opts->threads_per_source = it->second.threads_per_source;
         opts->chunk_sources = it->second.chunk_sources;
         opts->cached_closures = it->second.cached_closures;
+        opts->heavy_row = it->second.heavy_row;
         return GSOFA_OK;
     }
     if (cudaSetDevice(ctx->device) != cudaSuccess) return set_err(ctx, GSOFA_ERR_CUDA, "cudaSetDevice");
@@ -895,7 +896,8 @@ int gsofa_autotune(gsofa_ctx* ctx, const gsofa_matrix* mat, gsofa_opts* opts) {
         *ms = e ? 1e300 : r->counts.ms_traverse;
         return e;
     };
-    // coordinate descent from the defaults: CTA size, closure ring, chunk
+    // coordinate descent from the defaults: CTA size, closure ring, chunk,
+    // warp-walked row threshold
     gsofa_opts best = base;
     double best_ms = 0;
     rc = time_opts(best, &best_ms);
@@ -941,12 +943,24 @@ int gsofa_autotune(gsofa_ctx* ctx, const gsofa_matrix* mat, gsofa_opts* opts) {
             if (ms < best_ms) { best_ms = ms; best = p; }
         }
     }
+    // rows longer than this are walked by a whole warp
+    const int heavy_now = best.heavy_row > 0 ? best.heavy_row : kDefaultHeavyRow;
+    best.heavy_row = heavy_now;
+    for (int hr : {32, 64}) {
+        if (hr == heavy_now) continue;
+        gsofa_opts p = best;
+        p.heavy_row = hr;
+        double ms;
+        if ((rc = time_opts(p, &ms))) { result_free(r); return rc; }
+        if (ms < best_ms) { best_ms = ms; best = p; }
+    }
     (void)best_ms;
     result_free(r);
     ctx->tuned[key] = best;
     opts->threads_per_source = best.threads_per_source;
     opts->chunk_sources = best.chunk_sources;
     opts->cached_closures = best.cached_closures;
+    opts->heavy_row = best.heavy_row;
     return GSOFA_OK;
 }
 

@@ -130,7 +130,7 @@ size_t result_bytes(int32_t n, uint32_t flags);
 constexpr int kDefaultBuAlpha = 0;  // top-down only unless a caller asks
 constexpr int kDefaultBuBeta = 24;
 constexpr int kBuMinSource = 2048;
-constexpr int kDefaultHeavyRow = 64;
+constexpr int kDefaultHeavyRow = 16;  // padded rows above it are walked by a whole warp
 constexpr int kDefaultRing = 32;
 
 }  // namespace host

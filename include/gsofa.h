@@ -70,7 +70,7 @@ typedef struct gsofa_opts {
     int32_t bu_alpha;
     int32_t bu_beta;
     /* rows longer than this many entries are walked by a whole warp instead
-     * of one lane; 0 = default */
+     * of one lane; 0 = default (16) */
     int32_t heavy_row;
     /* sources with a smaller id always stay top-down; 0 = default (2048) */
     int32_t bu_min_source;
@@ -121,7 +121,7 @@ int gsofa_matrix_destroy(gsofa_matrix* mat);
 int gsofa_factor_symbolic(gsofa_ctx* ctx, const gsofa_matrix* mat, const gsofa_opts* opts,
                           gsofa_result** out);
 /* Autotuner: times candidate launch shapes (threads_per_source,
- * chunk_sources, cached_closures) for this matrix on a sample of its work
+ * chunk_sources, cached_closures, heavy_row) for this matrix on a sample of its work
  * and writes the fastest into *opts (other fields are left as given).
  * Results never depend on these settings.  Choices are cached in the
  * context per size class (log2 n, mean row length), so later calls for
