@@ -263,6 +263,7 @@ MatDesc make_desc(const gsofa_matrix* m, const gsofa_result* r, long long base) 
     d.wdeg = m->wdeg;
     d.dplanes = m->dplanes;
     d.nplanes = m->nplanes;
+    d.asym = m->asym;
     d.nnz_u = r->nnz_u;
     d.nz_row_u = r->nz_row_u;
     d.dig_u = r->dig_u;
@@ -491,6 +492,7 @@ bool gsofa::matrix_view(const void* mat, MatrixView* out) {
     out->wdeg = m->wdeg;
     out->dplanes = m->dplanes;
     out->nplanes = m->nplanes;
+    out->asym = m->asym;
     return true;
 }
 
@@ -499,7 +501,7 @@ void gsofa::host::ingest_bytes(int32_t n, int64_t nnz, size_t* kept, size_t* sta
     const size_t N1 = (size_t)n + 1;
     const size_t PT = (size_t)std::max<int64_t>(nnz + 3ll * n, 4);
     const size_t NW = (size_t)(((int64_t)n + 31) >> 5) + 1;
-    *kept = align256(4 * N1) * 2 + align256(4 * PT) * 2 + align256(4 * NW) * 32;
+    *kept = align256(4 * N1) * 2 + align256(4 * PT) * 2 + align256(4 * NW) * 32 + 256;
     const size_t Nin = (size_t)std::max<int64_t>(nnz, 1);
     *staging = align256(4 * N1) + align256(4 * Nin) + align256(4 * N1) * 3 +
                align256(canonicalize_scan_bytes(n)) + 256;
@@ -546,7 +548,7 @@ int gsofa::host::ingest_csr(gsofa_ctx* ctx, cudaStream_t stream, int32_t* dstatu
     while (nplanes < 32 && (maxd >> nplanes) != 0) nplanes++;
     m->nplanes = nplanes;
     size_t total = align256(4 * N1) * 2 + align256(4 * PA) + align256(4 * PT) + align256(4 * NW) +
-                   align256(4 * NW * (size_t)std::max(nplanes, 1));
+                   align256(4 * NW * (size_t)std::max(nplanes, 1)) + 256;
     void* blk = nullptr;
     int rc = dev_alloc_on(ctx, total, &blk, stream);
     if (rc) { delete m; return rc; }
@@ -560,6 +562,7 @@ int gsofa::host::ingest_csr(gsofa_ctx* ctx, cudaStream_t stream, int32_t* dstatu
                                          align256(4 * PT));
     m->dplanes = reinterpret_cast<uint32_t*>(b + 2 * align256(4 * N1) + align256(4 * PA) +
                                              align256(4 * PT) + align256(4 * NW));
+    m->asym = reinterpret_cast<int32_t*>(b + total - 256);
 
     // staging: raw input (beg, col_in) and the transpose's counters
     const size_t Nin = (size_t)std::max<int64_t>(nnz, 1);
@@ -604,8 +607,9 @@ int gsofa::host::ingest_csr(gsofa_ctx* ctx, cudaStream_t stream, int32_t* dstatu
     CKL(cudaMemsetAsync(tcount, 0, 4 * N1, stream));
     CKL(cudaMemsetAsync(tfill, 0, 4 * N1, stream));
     CKL(launch_canonicalize(n, nnz, dbeg, dcol_in, m->rowptr, m->col, tcount, tpad, m->trowptr,
-                            m->tcol, tfill, m->wdeg, m->dplanes, m->nplanes, scan_tmp,
-                            scan_bytes, dstatus, stream));
+                            m->tcol, tfill, m->wdeg, m->dplanes, m->nplanes, m->asym,
+                            maxd <= kSymmetryCheckMaxRow ? 1 : 0, scan_tmp, scan_bytes, dstatus,
+                            stream));
 #undef CKL
     dev_free_on(ctx, sblk, stage, stream);  // stream-ordered: after the build
     *out = m;

@@ -53,6 +53,7 @@ struct gsofa_matrix {
     int32_t* wdeg = nullptr;
     uint32_t* dplanes = nullptr;
     int32_t nplanes = 0;
+    int32_t* asym = nullptr;  // device word: 0 iff the pattern is symmetric
     size_t bytes = 0;
 };
 
@@ -132,6 +133,9 @@ constexpr int kDefaultBuBeta = 24;
 constexpr int kBuMinSource = 2048;
 constexpr int kDefaultHeavyRow = 16;  // padded rows above it are walked by a whole warp
 constexpr int kDefaultRing = 32;
+// rows longer than this skip the ingest's symmetry check (its cost grows with
+// the product of row lengths); such matrices are treated as unsymmetric
+constexpr int64_t kSymmetryCheckMaxRow = 8192;
 
 }  // namespace host
 }  // namespace gsofa

@@ -37,6 +37,10 @@ struct MatDesc {
     const uint32_t* dplanes;    // nplanes * ceil(n/32): degree bit-planes of A's rows
     int32_t nplanes;            // bits of A's largest row length
     int32_t pad0;
+    // 0 when A's pattern equals A^T's (set by the ingest's check): the L
+    // column searches in A^T then repeat the U row searches in A, and the
+    // direction-0 census writes both halves
+    const int32_t* asym;
     int32_t* nnz_u;             // n: |U row|
     int32_t* nz_row_u;          // n: reference nz_row_U counter
     uint64_t* dig_u;            // n (or null)
@@ -135,8 +139,8 @@ cudaError_t launch_canonicalize(int32_t n, long long nnz_in, const int32_t* beg,
                                 const int32_t* col_in, const int32_t* rp, int32_t* col_out,
                                 int32_t* tcount, int32_t* tpad, int32_t* trp, int32_t* tcol,
                                 int32_t* tfill, int32_t* wdeg, uint32_t* dplanes, int nplanes,
-                                void* scan_tmp, size_t scan_tmp_bytes, int32_t* status,
-                                cudaStream_t stream);
+                                int32_t* asym, int check_symmetry, void* scan_tmp,
+                                size_t scan_tmp_bytes, int32_t* status, cudaStream_t stream);
 size_t canonicalize_scan_bytes(int32_t n);
 cudaError_t launch_supernodes(int32_t n, int32_t mss, const int32_t* nz_row_u,
                               const uint32_t* lmask, int8_t* flags,
@@ -163,6 +167,7 @@ struct MatrixView {
     const int32_t* wdeg;
     const uint32_t* dplanes;
     int32_t nplanes;
+    const int32_t* asym;
 };
 bool matrix_view(const void* mat, MatrixView* out);
 

@@ -105,6 +105,7 @@ struct TraverseSmem {
     int skip;             // the current item's matrix failed ingest: count it only
     int cta;              // workspace slot (serving) or block index
     int wlo, whi;         // bitmap words holding the current source's set bits
+    int sym;              // the current item's matrix has a symmetric pattern
     int ring_lo[32];      // per ring slot: the words its closure occupies
     int ring_hi[32];
 };
@@ -649,6 +650,7 @@ __global__ void __launch_bounds__(BLOCK, 1024 / BLOCK) traverse_kernel(TraverseL
                     if (got) {
                         copy_desc<true>(&SD, P.serve.slots + slot);
                         SM.skip = __ldcg(P.serve.slot_status + slot) != 0;  // ingest failed
+                        SM.sym = SD.asym != nullptr && __ldcg(SD.asym) == 0;
                     }
                     SM.item = got ? it : -1;
                 }
@@ -660,6 +662,7 @@ __global__ void __launch_bounds__(BLOCK, 1024 / BLOCK) traverse_kernel(TraverseL
                 SM.mi = find_matrix(P.mats, P.nmats, it * stride);
                 copy_desc<false>(&SD, P.mats + SM.mi);
                 SM.skip = 0;
+                SM.sym = SD.asym != nullptr && *SD.asym == 0;
             }
             SM.item = it;
         }
@@ -675,7 +678,12 @@ __global__ void __launch_bounds__(BLOCK, 1024 / BLOCK) traverse_kernel(TraverseL
         const long long nchunks = ((long long)n + clen - 1) / clen;
         const long long chunk = nchunks - 1 - (local >> 1);  // largest sources first
         const int32_t s_first = (int32_t)(chunk * clen);
-        const int32_t s_end = SM.skip ? s_first : (int32_t)min((long long)n, (chunk + 1) * clen);
+        // symmetric pattern: the direction-0 item of this chunk does both halves
+        const bool sym = SM.sym != 0;
+        const bool lfold = sym && dir == 0;
+        const int32_t s_end = (SM.skip || (sym && dir == 1))
+                                  ? s_first
+                                  : (int32_t)min((long long)n, (chunk + 1) * clen);
         const long long words = bitmap_words_for(n);
         const long long nwords = ((long long)n + 31) >> 5;
         if constexpr (MODE == 2) bm = words <= P.serve.smem_words ? sbm : gbm;
@@ -696,7 +704,7 @@ __global__ void __launch_bounds__(BLOCK, 1024 / BLOCK) traverse_kernel(TraverseL
         S.ring = P.ring;
         S.abort_flag = &SM.abort_level;
         const bool digests = M.dig_u != nullptr;
-        const bool scatter = dir == 1 && M.nnz_lr != nullptr && !P.pattern_pass;
+        const bool scatter = (dir == 1 || lfold) && M.nnz_lr != nullptr && !P.pattern_pass;
 
         for (int32_t src = s_first; src < s_end; src++) {
             S.src = src;
@@ -815,7 +823,7 @@ __global__ void __launch_bounds__(BLOCK, 1024 / BLOCK) traverse_kernel(TraverseL
             __syncthreads();
             const long long wlo = SM.wlo, whi = SM.whi;
 
-            if (dir == 1 && !P.pattern_pass && threadIdx.x < 4) {
+            if ((dir == 1 || lfold) && !P.pattern_pass && threadIdx.x < 4) {
                 // 128-bit mask of rows f+1 .. f+128 in L column f (supernode test)
                 const long long p = (long long)src + 1 + 32 * threadIdx.x;
                 const long long wd = p >> 5;
@@ -828,6 +836,8 @@ __global__ void __launch_bounds__(BLOCK, 1024 / BLOCK) traverse_kernel(TraverseL
                 // sorted ids of the set bits > src: U row (dir 0) or L column (dir 1)
                 int32_t* out = dir == 0 ? M.ucols : M.lrows;
                 const long long obase = dir == 0 ? M.uptr[src] : M.lptr[src];
+                int32_t* out2 = lfold ? M.lrows : nullptr;  // the same ids: L column src
+                const long long obase2 = lfold ? M.lptr[src] : 0;
                 long long wpos = ((long long)src + 1) >> 5;
                 long long written = 0;
                 for (; wpos < nwords; wpos += BLOCK) {
@@ -844,10 +854,12 @@ __global__ void __launch_bounds__(BLOCK, 1024 / BLOCK) traverse_kernel(TraverseL
                     int cntw = __popc(word), ex = 0, tot = 0;
                     typename TraverseSmem<BLOCK>::Scan(SM.scan).ExclusiveSum(cntw, ex, tot);
                     long long o = obase + written + ex;
+                    long long o2 = obase2 + written + ex;
                     while (word) {
                         const int bpos = __ffs(word) - 1;
                         word &= word - 1;
                         out[o++] = (int32_t)((wi << 5) + bpos);
+                        if (out2) out2[o2++] = (int32_t)((wi << 5) + bpos);
                     }
                     written += tot;
                     __syncthreads();  // scan storage reuse
@@ -934,7 +946,8 @@ __global__ void __launch_bounds__(BLOCK, 1024 / BLOCK) traverse_kernel(TraverseL
                     M.nnz_u[src] = (int32_t)gt;
                     M.nz_row_u[src] = (int32_t)(rw + gt - og);
                     if (digests) M.dig_u[src] = r[5];
-                } else {
+                }
+                if (dir == 1 || lfold) {
                     M.nnz_lc[src] = (int32_t)gt;
                     if (digests) M.dig_lc[src] = r[5];
                 }
@@ -942,15 +955,14 @@ __global__ void __launch_bounds__(BLOCK, 1024 / BLOCK) traverse_kernel(TraverseL
                     if (acc_mat >= 0) flush_counters(P.mats[acc_mat].counters, acc);
                     acc_mat = mi;
                 }
-                acc[0] += gt - og;
+                acc[0] += (gt - og) * (lfold ? 2 : 1);  // symmetric: L fills = U fills
                 acc[3] += r[6];
                 if (dir == 0) {
                     acc[1] += ee;
                     acc[2] += vv;
                     acc[4] += gt;
-                } else {
-                    acc[5] += gt;
                 }
+                if (dir == 1 || lfold) acc[5] += gt;
             }
             __syncthreads();
         }
@@ -1172,6 +1184,29 @@ __global__ void word_degree_kernel(int32_t n, const int32_t* __restrict__ rp,
     }
 }
 
+// Pattern symmetry check, one warp per row: *asym becomes non-zero as soon
+// as an off-diagonal entry (v, w) has no (w, v).  Rows are unsorted, so each
+// lane scans row w; the caller skips the check (and marks the matrix
+// unsymmetric) when some row is longer than 8192 entries.
+__global__ void symmetry_kernel(int32_t n, const int32_t* __restrict__ rp,
+                                const int32_t* __restrict__ col, int32_t* asym) {
+    const int lane = threadIdx.x & 31;
+    const long long gw = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
+    for (long long v = gw; v < n; v += nwarps) {
+        if (*reinterpret_cast<volatile int32_t*>(asym)) return;
+        const int b = rp[v] & ~3, e = rp[v + 1] & ~3;  // padding entries repeat v
+        for (int k = b + lane; k < e; k += 32) {
+            const int w = col[k];
+            if (w == (int)v) continue;
+            const int wb = rp[w] & ~3, we = rp[w + 1] & ~3;
+            bool found = false;
+            for (int j = wb; j < we && !found; j++) found = col[j] == (int)v;
+            if (!found) atomicOr(asym, 1);
+        }
+    }
+}
+
 __global__ void transpose_pad_kernel(int32_t n, const int32_t* __restrict__ tcount,
                                      const int32_t* __restrict__ trp, int32_t* __restrict__ tcol) {
     for (long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x; c < n;
@@ -1194,8 +1229,10 @@ cudaError_t launch_canonicalize(int32_t n, long long nnz_in, const int32_t* beg,
                                 const int32_t* col_in, const int32_t* rp, int32_t* col_out,
                                 int32_t* tcount, int32_t* tpad, int32_t* trp, int32_t* tcol,
                                 int32_t* tfill, int32_t* wdeg, uint32_t* dplanes, int nplanes,
-                                void* scan_tmp, size_t scan_tmp_bytes, int32_t* status,
-                                cudaStream_t st) {
+                                int32_t* asym, int check_symmetry, void* scan_tmp,
+                                size_t scan_tmp_bytes, int32_t* status, cudaStream_t st) {
+    cudaError_t e0 = cudaMemsetAsync(asym, check_symmetry ? 0 : 1, 4, st);
+    if (e0 != cudaSuccess) return e0;
     if (n <= 0) return cudaSuccess;
     const int threads = 256;
     long long grid_w = ((long long)n * 32 + threads - 1) / threads;
@@ -1217,7 +1254,12 @@ cudaError_t launch_canonicalize(int32_t n, long long nnz_in, const int32_t* beg,
     transpose_pad_kernel<<<gridt, threads, 0, st>>>(n, tcount, trp, tcol);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
     word_degree_kernel<<<gridt, threads, 0, st>>>(n, rp, wdeg, dplanes, nplanes);
-    return cudaGetLastError();
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    if (check_symmetry) {
+        symmetry_kernel<<<grid, threads, 0, st>>>(n, rp, col_out, asym);
+        return cudaGetLastError();
+    }
+    return cudaSuccess;
 }
 
 // ---- supernodes: segmented compare-and-scan ---------------------------------

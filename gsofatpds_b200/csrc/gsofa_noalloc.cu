@@ -147,6 +147,7 @@ extern "C" int gsofa_factor_symbolic_noalloc(const gsofa_matrix* mat, const gsof
     d.wdeg = mv.wdeg;
     d.dplanes = mv.dplanes;
     d.nplanes = mv.nplanes;
+    d.asym = mv.asym;
     d.nnz_u = d_nnz_u_row;
     d.nz_row_u = d_nz_row_u;
     d.nnz_lc = d_nnz_l_col;

@@ -450,3 +450,41 @@ def test_reference_entry_point_and_cli(ctx, tmp_path):
     assert r.counts["fill_count"] == int(O.rows(b, e, col)["fills"].sum())
     r.close()
     m.close()
+
+
+def test_symmetric_pattern_shortcut(ctx):
+    """A symmetric pattern runs only the U-row searches (the L columns repeat
+    them); one extra unmatched entry turns the shortcut off.  Both must equal
+    the oracle, and the symmetric run inspects about half the entries."""
+    from gsofatpds_b200 import gen
+    _, rp, col = gen.grid_nd((14, 14, 14), "7")
+    n = rp.shape[0] - 1
+    beg, end = rp[:-1].copy(), rp[1:].copy()
+    # asymmetric twin: one more entry (v, w) without (w, v)
+    v, w = 5, n - 3
+    col2 = np.concatenate([col[:end[v]], [w], col[end[v]:]]).astype(np.int32)
+    beg2, end2 = beg.copy(), end.copy()
+    end2[v] += 1
+    beg2[v + 1:] += 1
+    end2[v + 1:] += 1
+    out = []
+    for b, e, c in [(beg, end, col), (beg2, end2, col2)]:
+        r, rt = oracle_full(b, e, c)
+        m = ctx.load_csr(b, e, c)
+        res = ctx.factor(m, l_row_stats=True)
+        check_full(res, r, rt)
+        out.append(res.counts["edges_traversed"])
+        res.close()
+        m.close()
+    assert out[0] * 1.5 < out[1], out
+    # duplicated entries and unsorted rows keep a symmetric pattern symmetric
+    rng = np.random.default_rng(7)
+    pat = random_pattern(rng, 60, 0.08, diag=True)
+    pat = [set(p) | {j for j in range(60) if i in pat[j]} for i, p in enumerate(pat)]
+    b, e, c = scrambled_csr(rng, pat, dup_prob=0.3)
+    r, rt = oracle_full(b, e, c)
+    m = ctx.load_csr(b, e, c)
+    res = ctx.factor(m, l_row_stats=True)
+    check_full(res, r, rt)
+    res.close()
+    m.close()
