@@ -307,7 +307,7 @@ int run_factor(gsofa_ctx* ctx, const gsofa_matrix* const* mats, int32_t count,
     }
     const bool merge = !(o->flags & GSOFA_NO_MERGE);
     int ring = o->cached_closures > 0 ? o->cached_closures : kDefaultRing;
-    if (ring > 32) ring = 32;
+    if (ring > kMaxRing) ring = kMaxRing;
     while (ring & (ring - 1)) ring &= ring - 1;  // power of 2
     if (merge) {
         rc = ensure(ctx, &ctx->gprev, &ctx->gprev_bytes,
@@ -920,7 +920,7 @@ int gsofa_autotune(gsofa_ctx* ctx, const gsofa_matrix* mat, gsofa_opts* opts) {
         if ((rc = time_opts(p, &ms))) { result_free(r); return rc; }
         if (ms < best_ms) { best_ms = ms; best = p; }
     }
-    const int ring_c[] = {1, 8, 32};
+    const int ring_c[] = {1, 8, 32, 64};
     const int ring_now = best.cached_closures > 0 ? best.cached_closures : kDefaultRing;
     best.cached_closures = ring_now;
     for (int ring : ring_c) {
@@ -1040,7 +1040,7 @@ int gsofa_batch_create(gsofa_ctx* ctx, const gsofa_matrix* const* mats, int32_t 
         o.chunk_sources > 0 ? o.chunk_sources : default_chunk(total_sources, cfg.grid);
     const bool merge = !(o.flags & GSOFA_NO_MERGE);
     int ring = o.cached_closures > 0 ? o.cached_closures : kDefaultRing;
-    if (ring > 32) ring = 32;
+    if (ring > kMaxRing) ring = kMaxRing;
     while (ring & (ring - 1)) ring &= ring - 1;
     // descriptors, segment prefix, counters, workspace: one private block
     std::vector<MatDesc> descs((size_t)count);

@@ -132,7 +132,8 @@ constexpr int kDefaultBuAlpha = 0;  // top-down only unless a caller asks
 constexpr int kDefaultBuBeta = 24;
 constexpr int kBuMinSource = 2048;
 constexpr int kDefaultHeavyRow = 16;  // padded rows above it are walked by a whole warp
-constexpr int kDefaultRing = 32;
+constexpr int kDefaultRing = 64;
+constexpr int kMaxRing = 64;  // the kernel's ring masks hold 64 slots
 // rows longer than this skip the ingest's symmetry check (its cost grows with
 // the product of row lengths); such matrices are treated as unsymmetric
 constexpr int64_t kSymmetryCheckMaxRow = 8192;

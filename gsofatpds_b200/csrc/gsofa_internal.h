@@ -109,7 +109,7 @@ struct TraverseLaunch {
     uint32_t* gprev;            // grid * ring * bitmap_words: each CTA's recent closures
     int chunk;                  // consecutive sources per work item
     int merge;                  // 1: reuse the closures of reached cached sources
-    int ring;                   // cached closures per CTA (power of 2, <= 32)
+    int ring;                   // cached closures per CTA (power of 2, <= 64)
     long long sample_stride;    // > 1: process only every stride-th item (autotuner timing)
     long long bitmap_words;     // words per bitmap (covers max n + padding)
     int32_t* status;            // device error word

@@ -89,6 +89,9 @@ __device__ __forceinline__ int row_degree(const int32_t* rp, int v) {
     return (b & ~3) - (a & ~3) - (b & 3);
 }
 
+// Ring slot masks: one bit per closure-ring slot (up to 64 slots).
+typedef unsigned long long rmask_t;
+
 template <int BLOCK>
 struct TraverseSmem {
     typedef cub::BlockScan<int, BLOCK> Scan;
@@ -99,15 +102,15 @@ struct TraverseSmem {
     int grab[3];          // per level (rotating): 32-vertex chunks of the frontier taken
     int abort_level;  // set when a cached source is reached: stop, merge, redo
     int pushed;       // ids a merge appended to the queue
-    unsigned pending; // cached sources a merge set (slots), for the next decision
-    unsigned reached[3];  // per level (rotating): cached sources first reached
+    rmask_t pending;      // cached sources a merge set (slots), for the next decision
+    rmask_t reached[3];   // per level (rotating): cached sources first reached
     int mi;               // matrix of the current item
     int skip;             // the current item's matrix failed ingest: count it only
     int cta;              // workspace slot (serving) or block index
     int wlo, whi;         // bitmap words holding the current source's set bits
     int sym;              // the current item's matrix has a symmetric pattern
-    int ring_lo[32];      // per ring slot: the words its closure occupies
-    int ring_hi[32];
+    int ring_lo[64];      // per ring slot: the words its closure occupies
+    int ring_hi[64];
 };
 
 // Bitmap words of a matrix of order n: n bits plus zero padding read by the
@@ -134,11 +137,11 @@ struct Src {
     long long mwords;                 // this matrix's bitmap words (what a merge ORs)
     int ring;
     int32_t cache_lo;
-    uint32_t merged_mask;
+    rmask_t merged_mask;
     int top;                          // slot of the largest merged source, -1 if none
-    uint32_t pending;                 // cached sources a merge set, not yet merged (slots)
+    rmask_t pending;                  // cached sources a merge set, not yet merged (slots)
     int* abort_flag;
-    unsigned* reached;                // slots of cached sources first reached this level
+    rmask_t* reached;                 // slots of cached sources first reached this level
 };
 
 // The cached source held in ring slot j.
@@ -160,7 +163,7 @@ __device__ __forceinline__ bool covered(const Src& S, int top, int32_t v) {
 }
 
 // Slot of the largest source in a merged mask, or -1.
-__device__ __forceinline__ int top_slot(const Src& S, uint32_t mask) {
+__device__ __forceinline__ int top_slot(const Src& S, rmask_t mask) {
     for (int32_t t = S.src - 1; t >= S.cache_lo; t--)
         if ((mask >> (t & (S.ring - 1))) & 1u) return t & (S.ring - 1);
     return -1;
@@ -189,7 +192,7 @@ __device__ __forceinline__ bool td_edge(const Src& S, int v, int w, uint32_t& ra
         return false;
     }
     if (fresh && w >= S.cache_lo && !((S.merged_mask >> (w & (S.ring - 1))) & 1u)) {
-        atomicOr(S.reached, 1u << (w & (S.ring - 1)));
+        atomicOr(S.reached, 1ull << (w & (S.ring - 1)));
         *(volatile int*)S.abort_flag = 1;
     }
     return fresh;
@@ -249,18 +252,26 @@ __device__ __forceinline__ void td_level(const Src& S, int32_t* q, long long qca
     // warps take 32-vertex chunks of the frontier as they free up: rows of
     // very uneven length would leave statically assigned warps idle at the
     // level's barrier
+    int chunk0 = 0;
+    if (lane == 0) chunk0 = atomicAdd(grab, 1);
+    long long nbase = lb + 32ll * __shfl_sync(FULL_MASK, chunk0, 0);
+    int nv = (nbase + lane < le) ? q[nbase + lane] : S.src;
     for (;;) {
+        const long long base = nbase;
+        if (base >= le) break;
+        const long long i = base + lane;
+        int v = nv;
+        // take the next chunk and start loading its entries now: the queue
+        // round trip overlaps this chunk's work
         int chunk = 0;
         if (lane == 0) chunk = atomicAdd(grab, 1);
-        const long long base = lb + 32ll * __shfl_sync(FULL_MASK, chunk, 0);
-        if (base >= le) break;
+        nbase = lb + 32ll * __shfl_sync(FULL_MASK, chunk, 0);
+        nv = (nbase + lane < le) ? q[nbase + lane] : S.src;
         // stop when a cached source was reached; one value for the whole warp
         const int ab = __shfl_sync(FULL_MASK, *(volatile int*)S.abort_flag, 0);
         if (lb > 0 && ab) break;
-        const long long i = base + lane;
-        int v = S.src, s0 = 0, plen = 0;
+        int s0 = 0, plen = 0;
         if (i < le) {
-            v = q[i];
             bool skip = false;
             if (S.merged_mask) skip = v == S.src || covered(S, S.top, v);
             if (!skip) {
@@ -351,7 +362,7 @@ __device__ __forceinline__ void bu_sweep(const Src& S, bool upper, int32_t* q, l
                 const long long at = le + base + __popc(bal & ((1u << lane) - 1u));
                 if (at < qcap) q[at] = (int32_t)u;
                 else atomicOr(status, DEV_ERR_QUEUE);
-                if (u >= S.cache_lo) atomicOr(S.reached, 1u << ((int)u & (S.ring - 1)));
+                if (u >= S.cache_lo) atomicOr(S.reached, 1ull << ((int)u & (S.ring - 1)));
             }
         }
     }
@@ -365,56 +376,57 @@ __device__ __forceinline__ void bu_sweep(const Src& S, bool upper, int32_t* q, l
 // appended to the queue at `at` (*pushed gets their number).  Block-wide,
 // uniform; returns the new merged mask.
 template <int BLOCK>
-__device__ __forceinline__ uint32_t merge_reached(const Src& S, uint32_t reached, uint32_t* bm,
+__device__ __forceinline__ rmask_t merge_reached(const Src& S, rmask_t reached, uint32_t* bm,
                                                   int32_t* q, long long at, long long qcap,
-                                                  int* pushed, uint32_t* pending_out,
+                                                  int* pushed, rmask_t* pending_out,
                                                   int32_t* status, bool& did_merge, int& wl,
                                                   int& wh) {
     // The decision uses only values every thread holds identically: the
     // level's reached mask (stable until two levels later), the pending mask
     // and the ring, never the live bitmap.
-    uint32_t add = 0;
+    rmask_t add = 0;
     did_merge = false;
-    uint32_t mm = S.merged_mask;
-    const uint32_t cand = (reached | S.pending) & ~mm;
+    rmask_t mm = S.merged_mask;
+    const rmask_t cand = (reached | S.pending) & ~mm;
     if (!cand) return mm;
     for (int32_t t = S.src - 1; t >= S.cache_lo; t--) {
         const int slot = t & (S.ring - 1);
         if (!((cand >> slot) & 1u)) continue;
         const bool inside = covered(S, top_slot(S, mm), t);
-        mm |= 1u << slot;
-        if (!inside) add |= 1u << slot;
+        mm |= 1ull << slot;
+        if (!inside) add |= 1ull << slot;
     }
     if (!add) return mm;
     did_merge = true;
     // ids in (t, src) of an added t's closure were never expanded; with only
     // src-1 added that window is empty and the merge is a plain OR
     int32_t lo = S.src;
-    for (uint32_t a = add; a; a &= a - 1) {
-        const int32_t t = slot_source(S, __ffs(a) - 1);
+    for (rmask_t a = add; a; a &= a - 1) {
+        const int32_t t = slot_source(S, __ffsll((long long)a) - 1);
         if (t + 1 < lo) lo = t + 1;
     }
     const bool window = lo < S.src;
-    // the window [lo, src) spans at most 32 ids: two words before the merge
+    // the window [lo, src) spans at most 63 ids: three words before the merge
     const long long w0 = lo >> 5, w1 = (S.src - 1) >> 5;
-    uint32_t b0 = 0, b1 = 0;
+    uint32_t b0 = 0, b1 = 0, b2 = 0;
     if (window) {
         b0 = ld_vol(bm + w0);
-        b1 = ld_vol(bm + w1);
+        if (w0 + 1 <= w1) b1 = ld_vol(bm + w0 + 1);
+        if (w0 + 2 <= w1) b2 = ld_vol(bm + w0 + 2);
         __syncthreads();
     }
     // OR the added closures over the words they occupy, four words per
     // thread per pass so that their loads overlap
     int mlo = INT_MAX, mhi = -1;
-    for (uint32_t a = add; a; a &= a - 1) {
-        const int sl = __ffs(a) - 1;
+    for (rmask_t a = add; a; a &= a - 1) {
+        const int sl = __ffsll((long long)a) - 1;
         mlo = min(mlo, S.ring_lo[sl]);
         mhi = max(mhi, S.ring_hi[sl]);
     }
     for (long long i0 = (long long)mlo + threadIdx.x; i0 <= mhi; i0 += 4ll * BLOCK) {
         uint32_t y[4] = {0u, 0u, 0u, 0u};
-        for (uint32_t a = add; a; a &= a - 1) {
-            const int sl = __ffs(a) - 1;
+        for (rmask_t a = add; a; a &= a - 1) {
+            const int sl = __ffsll((long long)a) - 1;
             const int slo = S.ring_lo[sl], shi = S.ring_hi[sl];
             const uint32_t* src = S.ring_base + (long long)sl * S.words;
 #pragma unroll
@@ -434,22 +446,22 @@ __device__ __forceinline__ uint32_t merge_reached(const Src& S, uint32_t reached
     if (!window) {
         if (threadIdx.x == 0) {
             *pushed = 0;
-            *pending_out = 0u;
+            *pending_out = 0ull;
         }
         return mm;  // the caller's barrier completes the merge
     }
     __syncthreads();
     if (threadIdx.x == 0) {
         int np = 0;
-        uint32_t pend = 0;
+        rmask_t pend = 0;
         const int top = top_slot(S, mm);
         for (int32_t v = lo; v < S.src; v++) {
             const long long w = v >> 5;
-            const uint32_t before = w == w0 ? b0 : b1;
+            const uint32_t before = w == w0 ? b0 : (w == w0 + 1 ? b1 : b2);
             const uint32_t bit = 1u << (v & 31);
             if ((before & bit) || !(ld_vol(bm + w) & bit)) continue;  // not set by the merge
             // a cached source set by the merge is reached too: merge it next time
-            if (!((mm >> (v & (S.ring - 1))) & 1u)) pend |= 1u << (v & (S.ring - 1));
+            if (!((mm >> (v & (S.ring - 1))) & 1ull)) pend |= 1ull << (v & (S.ring - 1));
             if (covered(S, top, v)) continue;
             if (at + np < qcap) q[at + np] = v;
             else atomicOr(status, DEV_ERR_QUEUE);
@@ -710,16 +722,16 @@ __global__ void __launch_bounds__(BLOCK, 1024 / BLOCK) traverse_kernel(TraverseL
             S.src = src;
             // cached: the last `ring` sources of this chunk (none without merging)
             S.cache_lo = P.merge ? max(s_first, src - P.ring) : src;
-            S.merged_mask = 0u;
+            S.merged_mask = 0ull;
             S.top = -1;
-            S.pending = 0u;
+            S.pending = 0ull;
             S.reached = &SM.reached[0];
             if (threadIdx.x == 0) {
                 bm[src >> 5] |= 1u << (src & 31);
                 q[0] = src;
                 SM.cnt[0] = 0;
                 SM.grab[0] = 0;
-                SM.reached[0] = 0u;
+                SM.reached[0] = 0ull;
                 SM.abort_level = 0;
                 SM.wlo = SM.whi = src >> 5;
             }
@@ -743,7 +755,7 @@ __global__ void __launch_bounds__(BLOCK, 1024 / BLOCK) traverse_kernel(TraverseL
                     if (threadIdx.x == 0) {
                         SM.cnt[(level + 1) % 3] = 0;
                         SM.grab[(level + 1) % 3] = 0;
-                        SM.reached[(level + 1) % 3] = 0u;
+                        SM.reached[(level + 1) % 3] = 0ull;
                     }
                     S.reached = &SM.reached[level % 3];
                     td_level<BLOCK, CG>(S, q, qcap, lb, le, &SM.cnt[level % 3], &SM.grab[level % 3],
@@ -753,8 +765,8 @@ __global__ void __launch_bounds__(BLOCK, 1024 / BLOCK) traverse_kernel(TraverseL
                     level++;
                     // a reached cached source's closure is ours: merge it
                     bool did = false;
-                    const uint32_t reached = SM.reached[(level - 1) % 3];
-                    const uint32_t mm =
+                    const rmask_t reached = SM.reached[(level - 1) % 3];
+                    const rmask_t mm =
                         S.cache_lo < src
                             ? merge_reached<BLOCK>(S, reached, bm, q, le + nxt, qcap, &SM.pushed,
                                                    &SM.pending, P.status, did, wl, wh)
@@ -777,7 +789,7 @@ __global__ void __launch_bounds__(BLOCK, 1024 / BLOCK) traverse_kernel(TraverseL
                     if (threadIdx.x == 0) {
                         SM.cnt[(level + 1) % 3] = 0;
                         SM.grab[(level + 1) % 3] = 0;
-                        SM.reached[(level + 1) % 3] = 0u;
+                        SM.reached[(level + 1) % 3] = 0ull;
                     }
                     S.reached = &SM.reached[level % 3];
                     bu_sweep<BLOCK, CG>(S, false, q, qcap, le, &SM.cnt[level % 3], P.status, trav);
@@ -788,8 +800,8 @@ __global__ void __launch_bounds__(BLOCK, 1024 / BLOCK) traverse_kernel(TraverseL
                     le = le + found;
                     if (le > qcap) le = qcap;
                     bool did = false;
-                    const uint32_t reached = SM.reached[(level - 1) % 3];
-                    const uint32_t mm =
+                    const rmask_t reached = SM.reached[(level - 1) % 3];
+                    const rmask_t mm =
                         S.cache_lo < src
                             ? merge_reached<BLOCK>(S, reached, bm, q, le, qcap, &SM.pushed,
                                                    &SM.pending, P.status, did, wl, wh)

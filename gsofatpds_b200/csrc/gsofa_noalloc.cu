@@ -110,7 +110,7 @@ extern "C" int gsofa_factor_symbolic_noalloc(const gsofa_matrix* mat, const gsof
 
     const bool merge = !(o.flags & GSOFA_NO_MERGE);
     int ring = o.cached_closures > 0 ? o.cached_closures : 8;
-    if (ring > 32) ring = 32;
+    if (ring > 64) ring = 64;  // the kernel's ring masks hold 64 slots
     while (ring & (ring - 1)) ring &= ring - 1;
     const long long chunk = o.chunk_sources > 0 ? o.chunk_sources : 64;
 

@@ -663,7 +663,7 @@ int gsofa_server_create(gsofa_ctx* ctx, const gsofa_opts* opts, int32_t max_n,
     s->budget = budget_bytes ? budget_bytes : kDefaultBudget;
     s->block = block;
     s->merge = !(o.flags & GSOFA_NO_MERGE);
-    s->ring = o.cached_closures > 0 ? std::min(o.cached_closures, 32) : kDefaultRing;
+    s->ring = o.cached_closures > 0 ? std::min(o.cached_closures, kMaxRing) : kDefaultRing;
     while (s->ring & (s->ring - 1)) s->ring &= s->ring - 1;
     s->t0 = std::chrono::steady_clock::now();
     auto fail = [&](int rc, const char* what, cudaError_t e) {

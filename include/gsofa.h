@@ -78,7 +78,7 @@ typedef struct gsofa_opts {
      * closure is reused inside a chunk); 0 = default */
     int32_t chunk_sources;
     /* closures of recently finished sources each CTA keeps for reuse
-     * (rounded down to a power of 2, at most 32); 0 = default */
+     * (rounded down to a power of 2, at most 64); 0 = default */
     int32_t cached_closures;
     int32_t reserved[2];
 } gsofa_opts;
