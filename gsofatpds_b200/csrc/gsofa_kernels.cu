@@ -398,6 +398,23 @@ __device__ __forceinline__ rmask_t merge_reached(const Src& S, rmask_t reached, 
     }
     if (!add) return mm;
     did_merge = true;
+    // stream the added closures into L2 at once with the bulk-copy engine;
+    // the loads below then hit L2 instead of waiting on DRAM a few lines at
+    // a time (16-byte-aligned interior only, so nothing outside the closure
+    // is touched)
+    if (threadIdx.x == 0) {
+        for (rmask_t a = add; a; a &= a - 1) {
+            const int sl = __ffsll((long long)a) - 1;
+            const uint32_t* p0 = S.ring_base + (long long)sl * S.words + S.ring_lo[sl];
+            const uint32_t* p1 = S.ring_base + (long long)sl * S.words + S.ring_hi[sl] + 1;
+            const unsigned long long a0 = (reinterpret_cast<unsigned long long>(p0) + 15ull) & ~15ull;
+            const unsigned long long a1 = reinterpret_cast<unsigned long long>(p1) & ~15ull;
+            if (a1 > a0)
+                asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(a0),
+                             "r"((unsigned)(a1 - a0))
+                             : "memory");
+        }
+    }
     // ids in (t, src) of an added t's closure were never expanded; with only
     // src-1 added that window is empty and the merge is a plain OR
     int32_t lo = S.src;
