@@ -925,7 +925,7 @@ __global__ void __launch_bounds__(BLOCK, 1024 / BLOCK) traverse_kernel(TraverseL
                 if (dir == 0 && xl) {
                     if (xl == ~0u) {
                         c_e += (unsigned long long)ld_i32<CG>(M.wdeg + w);
-                    } else if (__popc(xl) <= 4 || M.dplanes == nullptr) {
+                    } else if (__popc(xl) <= 2 || M.dplanes == nullptr) {
                         uint32_t t = xl;
                         while (t) {
                             const int bp = __ffs(t) - 1;
@@ -933,11 +933,19 @@ __global__ void __launch_bounds__(BLOCK, 1024 / BLOCK) traverse_kernel(TraverseL
                             c_e += (unsigned long long)row_degree<CG>(M.rowptr, (int)(base + bp));
                         }
                     } else {
-                        // degree sum from the bit-planes: a few coalesced loads
+                        // degree sum from the bit-planes: coalesced loads, four
+                        // issued before any is used
                         const int32_t* pl = reinterpret_cast<const int32_t*>(M.dplanes) + w;
-                        for (int k = 0; k < M.nplanes; k++)
-                            c_e += (unsigned long long)__popc(xl & (uint32_t)ld_i32<CG>(pl + k * nwords))
-                                   << k;
+                        const int np = M.nplanes;
+                        for (int k = 0; k < np; k += 4) {
+                            uint32_t p4[4];
+#pragma unroll
+                            for (int j = 0; j < 4; j++)
+                                p4[j] = k + j < np ? (uint32_t)ld_i32<CG>(pl + (k + j) * nwords) : 0u;
+#pragma unroll
+                            for (int j = 0; j < 4; j++)
+                                c_e += (unsigned long long)__popc(xl & p4[j]) << (k + j);
+                        }
                     }
                 }
                 c_gt += __popc(xh);
