@@ -389,10 +389,34 @@ __device__ __forceinline__ rmask_t merge_reached(const Src& S, rmask_t reached, 
     rmask_t mm = S.merged_mask;
     const rmask_t cand = (reached | S.pending) & ~mm;
     if (!cand) return mm;
-    for (int32_t t = S.src - 1; t >= S.cache_lo; t--) {
-        const int slot = t & (S.ring - 1);
-        if (!((cand >> slot) & 1u)) continue;
+    // Candidates in decreasing source order, each tested against the largest
+    // source marked so far.  After the first candidate is marked that source
+    // no longer changes (every later candidate is smaller), and all
+    // candidates lie in [cache_lo, src), at most three words: load those
+    // words of its closure once and test the rest with register bit tests.
+    int32_t t = S.src - 1;
+    while (t >= S.cache_lo && !((cand >> (t & (S.ring - 1))) & 1ull)) t--;
+    {
         const bool inside = covered(S, top_slot(S, mm), t);
+        mm |= 1ull << (t & (S.ring - 1));
+        if (!inside) add |= 1ull << (t & (S.ring - 1));
+    }
+    const int top = top_slot(S, mm);
+    const int32_t tsrc = slot_source(S, top);
+    const long long wb = S.cache_lo >> 5;
+    uint32_t cw[3] = {0u, 0u, 0u};
+#pragma unroll
+    for (int j = 0; j < 3; j++) {
+        const long long w = wb + j;
+        if (w <= ((S.src - 1) >> 5) && w >= S.ring_lo[top] && w <= S.ring_hi[top])
+            cw[j] = S.ring_base[(long long)top * S.words + w];
+    }
+    for (t = t - 1; t >= S.cache_lo; t--) {
+        const int slot = t & (S.ring - 1);
+        if (!((cand >> slot) & 1ull)) continue;
+        const int j = (int)((t >> 5) - wb);
+        const uint32_t word = j == 0 ? cw[0] : (j == 1 ? cw[1] : cw[2]);
+        const bool inside = t <= tsrc && ((word >> (t & 31)) & 1u);
         mm |= 1ull << slot;
         if (!inside) add |= 1ull << slot;
     }
