@@ -40,7 +40,7 @@ EXPORTS = [
     "gsofa_autotune", "gsofa_batch_create", "gsofa_batch_run", "gsofa_batch_result",
     "gsofa_batch_destroy", "gsofa_server_create", "gsofa_server_submit", "gsofa_server_poll",
     "gsofa_server_wait", "gsofa_server_ticket_info", "gsofa_server_get_stats",
-    "gsofa_server_destroy", "gsofa_server_last_error",
+    "gsofa_server_destroy", "gsofa_server_last_error", "gsofa_autotune_batch",
 ]
 
 
@@ -118,6 +118,7 @@ def load():
         "gsofa_result_pattern_l": [vp, vp, vp, i64],
         "gsofa_result_destroy": [vp],
         "gsofa_autotune": [vp, vp, ctypes.POINTER(Opts)],
+        "gsofa_autotune_batch": [vp, ctypes.POINTER(vp), i32, ctypes.POINTER(Opts)],
         "gsofa_batch_create": [vp, ctypes.POINTER(vp), i32, ctypes.POINTER(Opts), ctypes.POINTER(vp)],
         "gsofa_batch_run": [vp],
         "gsofa_batch_result": [vp, i32, ctypes.POINTER(vp)],

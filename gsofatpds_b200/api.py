@@ -110,6 +110,15 @@ class Context:
         return dict(threads_per_source=o.threads_per_source, chunk_sources=o.chunk_sources,
                     cached_closures=o.cached_closures, heavy_row=o.heavy_row)
 
+    def autotune_batch(self, mats, **kw):
+        """Fastest launch shape for one persistent launch over all `mats`."""
+        o = self.opts(**kw)
+        k = len(mats)
+        arr = (ctypes.c_void_p * max(k, 1))(*[m.handle for m in mats])
+        self._check(self._L.gsofa_autotune_batch(self._h, arr, k, ctypes.byref(o)), "autotune_batch")
+        return dict(threads_per_source=o.threads_per_source, chunk_sources=o.chunk_sources,
+                    cached_closures=o.cached_closures, heavy_row=o.heavy_row)
+
     def factor(self, mat, **kw):
         o = self.opts(**kw)
         h = ctypes.c_void_p()

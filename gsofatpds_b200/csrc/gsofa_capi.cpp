@@ -848,6 +848,122 @@ int gsofa_factor_batch(gsofa_ctx* ctx, const gsofa_matrix* const* mats, int32_t 
 // work items (large matrices) or on the whole matrix (small ones) and keeps
 // the fastest.  The candidates differ only in speed: every setting gives the
 // same results.  Choices are cached per size class in the context.
+// Coordinate descent over the launch shape (CTA size, closure ring, chunk,
+// warp-walked row threshold), each candidate timed on the device as one
+// persistent launch over all `count` matrices.  Writes the best into *opts.
+static int autotune_impl(gsofa_ctx* ctx, const gsofa_matrix* const* mats, int32_t count,
+                         gsofa_opts* opts) {
+    int rc = GSOFA_OK;
+    int32_t nmax = 0;
+    long long total_sources = 0;
+    for (int32_t i = 0; i < count; i++) {
+        nmax = std::max(nmax, mats[i]->n);
+        total_sources += 2ll * mats[i]->n;
+    }
+    if (cudaSetDevice(ctx->device) != cudaSuccess) return set_err(ctx, GSOFA_ERR_CUDA, "cudaSetDevice");
+    gsofa_opts base = *opts;
+    base.flags &= ~(uint32_t)(GSOFA_SUPERNODES | GSOFA_PATTERN | GSOFA_L_ROW_STATS);
+    // reference timing with the defaults picks the sampling rate
+    std::vector<gsofa_result*> rr((size_t)count, nullptr);
+    auto free_all = [&]() {
+        for (gsofa_result* x : rr) result_free(x);
+    };
+    for (int32_t i = 0; i < count; i++) {
+        rc = result_alloc(ctx, mats[i]->n, base.flags, base.max_supernode_size, &rr[(size_t)i]);
+        if (rc) { free_all(); return rc; }
+    }
+    rc = run_factor(ctx, mats, count, &base, rr.data());
+    if (rc) { free_all(); return rc; }
+    const double full_ms = rr[0]->counts.ms_traverse;  // the launch's time
+    // Full runs while they are short; above 2 s time every stride-th work
+    // item, keeping at least 16 items per CTA so the tail does not dominate.
+    long long stride = 1;
+    if (full_ms > 2000.0) {
+        LaunchCfg c0;
+        if (plan_launch(ctx, nmax, &base, &c0) == GSOFA_OK) {
+            const long long items = total_sources / 16 + 2ll * count;
+            stride = (long long)(full_ms / 1000.0);
+            while (stride > 1 && items / stride < 16ll * c0.grid) stride--;
+        }
+    }
+    auto time_opts = [&](const gsofa_opts& p, double* ms) -> int {
+        LaunchCfg c;
+        if (plan_launch(ctx, nmax, &p, &c) != GSOFA_OK) {
+            ctx->err.clear();
+            *ms = 1e300;
+            return GSOFA_OK;
+        }
+        int e = run_factor(ctx, mats, count, &p, rr.data(), stride);
+        *ms = e ? 1e300 : rr[0]->counts.ms_traverse;
+        return e;
+    };
+    // coordinate descent from the defaults: CTA size, closure ring, chunk,
+    // warp-walked row threshold
+    gsofa_opts best = base;
+    double best_ms = 0;
+    rc = time_opts(best, &best_ms);
+    if (rc) { free_all(); return rc; }
+    {
+        LaunchCfg c0;
+        if (plan_launch(ctx, nmax, &base, &c0) == GSOFA_OK) best.threads_per_source = c0.block;
+        ctx->err.clear();
+    }
+    const int tps_c[] = {256, 512, 1024};
+    for (int tps : tps_c) {
+        if (tps == best.threads_per_source) continue;
+        gsofa_opts p = best;
+        p.threads_per_source = tps;
+        double ms;
+        if ((rc = time_opts(p, &ms))) { free_all(); return rc; }
+        if (ms < best_ms) { best_ms = ms; best = p; }
+    }
+    const int ring_c[] = {1, 8, 32, 64};
+    const int ring_now = best.cached_closures > 0 ? best.cached_closures : kDefaultRing;
+    best.cached_closures = ring_now;
+    for (int ring : ring_c) {
+        if (ring == ring_now) continue;
+        gsofa_opts p = best;
+        p.cached_closures = ring;
+        double ms;
+        if ((rc = time_opts(p, &ms))) { free_all(); return rc; }
+        if (ms < best_ms) { best_ms = ms; best = p; }
+    }
+    {
+        LaunchCfg c;
+        long long auto_chunk = 64;
+        if (plan_launch(ctx, nmax, &best, &c) == GSOFA_OK) auto_chunk = default_chunk(total_sources, c.grid);
+        ctx->err.clear();
+        if (best.chunk_sources <= 0) best.chunk_sources = (int32_t)auto_chunk;
+        const long long cands[] = {auto_chunk / 4, auto_chunk * 2};
+        for (long long ch : cands) {
+            if (ch < 16 || ch > 1024 || ch == best.chunk_sources) continue;
+            gsofa_opts p = best;
+            p.chunk_sources = (int32_t)ch;
+            double ms;
+            if ((rc = time_opts(p, &ms))) { free_all(); return rc; }
+            if (ms < best_ms) { best_ms = ms; best = p; }
+        }
+    }
+    // rows longer than this are walked by a whole warp
+    const int heavy_now = best.heavy_row > 0 ? best.heavy_row : kDefaultHeavyRow;
+    best.heavy_row = heavy_now;
+    for (int hr : {32, 64}) {
+        if (hr == heavy_now) continue;
+        gsofa_opts p = best;
+        p.heavy_row = hr;
+        double ms;
+        if ((rc = time_opts(p, &ms))) { free_all(); return rc; }
+        if (ms < best_ms) { best_ms = ms; best = p; }
+    }
+    (void)best_ms;
+    free_all();
+    opts->threads_per_source = best.threads_per_source;
+    opts->chunk_sources = best.chunk_sources;
+    opts->cached_closures = best.cached_closures;
+    opts->heavy_row = best.heavy_row;
+    return GSOFA_OK;
+}
+
 int gsofa_autotune(gsofa_ctx* ctx, const gsofa_matrix* mat, gsofa_opts* opts) {
     if (!ctx || !mat || !opts || mat->ctx != ctx) return GSOFA_ERR_ARG;
     std::lock_guard<std::recursive_mutex> g(ctx->mu);
@@ -866,106 +982,24 @@ int gsofa_autotune(gsofa_ctx* ctx, const gsofa_matrix* mat, gsofa_opts* opts) {
         opts->heavy_row = it->second.heavy_row;
         return GSOFA_OK;
     }
-    if (cudaSetDevice(ctx->device) != cudaSuccess) return set_err(ctx, GSOFA_ERR_CUDA, "cudaSetDevice");
-    gsofa_opts base = *opts;
-    base.flags &= ~(uint32_t)(GSOFA_SUPERNODES | GSOFA_PATTERN | GSOFA_L_ROW_STATS);
-    // reference timing with the defaults picks the sampling rate
-    gsofa_result* r = nullptr;
-    rc = result_alloc(ctx, mat->n, base.flags, base.max_supernode_size, &r);
-    if (rc) return rc;
     const gsofa_matrix* const mats[1] = {mat};
-    gsofa_result* rr[1] = {r};
-    rc = run_factor(ctx, mats, 1, &base, rr);
-    if (rc) { result_free(r); return rc; }
-    const double full_ms = r->counts.ms_traverse;
-    // Full runs while they are short; above 2 s time every stride-th work
-    // item, keeping at least 16 items per CTA so the tail does not dominate.
-    long long stride = 1;
-    if (full_ms > 2000.0) {
-        LaunchCfg c0;
-        if (plan_launch(ctx, mat->n, &base, &c0) == GSOFA_OK) {
-            const long long items = 2ll * (mat->n / 16 + 1);
-            stride = (long long)(full_ms / 1000.0);
-            while (stride > 1 && items / stride < 16ll * c0.grid) stride--;
-        }
-    }
-    auto time_opts = [&](const gsofa_opts& p, double* ms) -> int {
-        LaunchCfg c;
-        if (plan_launch(ctx, mat->n, &p, &c) != GSOFA_OK) {
-            ctx->err.clear();
-            *ms = 1e300;
-            return GSOFA_OK;
-        }
-        int e = run_factor(ctx, mats, 1, &p, rr, stride);
-        *ms = e ? 1e300 : r->counts.ms_traverse;
-        return e;
-    };
-    // coordinate descent from the defaults: CTA size, closure ring, chunk,
-    // warp-walked row threshold
-    gsofa_opts best = base;
-    double best_ms = 0;
-    rc = time_opts(best, &best_ms);
-    if (rc) { result_free(r); return rc; }
-    {
-        LaunchCfg c0;
-        if (plan_launch(ctx, mat->n, &base, &c0) == GSOFA_OK) best.threads_per_source = c0.block;
-        ctx->err.clear();
-    }
-    const int tps_c[] = {256, 512, 1024};
-    for (int tps : tps_c) {
-        if (tps == best.threads_per_source) continue;
-        gsofa_opts p = best;
-        p.threads_per_source = tps;
-        double ms;
-        if ((rc = time_opts(p, &ms))) { result_free(r); return rc; }
-        if (ms < best_ms) { best_ms = ms; best = p; }
-    }
-    const int ring_c[] = {1, 8, 32, 64};
-    const int ring_now = best.cached_closures > 0 ? best.cached_closures : kDefaultRing;
-    best.cached_closures = ring_now;
-    for (int ring : ring_c) {
-        if (ring == ring_now) continue;
-        gsofa_opts p = best;
-        p.cached_closures = ring;
-        double ms;
-        if ((rc = time_opts(p, &ms))) { result_free(r); return rc; }
-        if (ms < best_ms) { best_ms = ms; best = p; }
-    }
-    {
-        LaunchCfg c;
-        long long auto_chunk = 64;
-        if (plan_launch(ctx, mat->n, &best, &c) == GSOFA_OK) auto_chunk = default_chunk(2ll * mat->n, c.grid);
-        ctx->err.clear();
-        if (best.chunk_sources <= 0) best.chunk_sources = (int32_t)auto_chunk;
-        const long long cands[] = {auto_chunk / 4, auto_chunk * 2};
-        for (long long ch : cands) {
-            if (ch < 16 || ch > 1024 || ch == best.chunk_sources) continue;
-            gsofa_opts p = best;
-            p.chunk_sources = (int32_t)ch;
-            double ms;
-            if ((rc = time_opts(p, &ms))) { result_free(r); return rc; }
-            if (ms < best_ms) { best_ms = ms; best = p; }
-        }
-    }
-    // rows longer than this are walked by a whole warp
-    const int heavy_now = best.heavy_row > 0 ? best.heavy_row : kDefaultHeavyRow;
-    best.heavy_row = heavy_now;
-    for (int hr : {32, 64}) {
-        if (hr == heavy_now) continue;
-        gsofa_opts p = best;
-        p.heavy_row = hr;
-        double ms;
-        if ((rc = time_opts(p, &ms))) { result_free(r); return rc; }
-        if (ms < best_ms) { best_ms = ms; best = p; }
-    }
-    (void)best_ms;
-    result_free(r);
-    ctx->tuned[key] = best;
-    opts->threads_per_source = best.threads_per_source;
-    opts->chunk_sources = best.chunk_sources;
-    opts->cached_closures = best.cached_closures;
-    opts->heavy_row = best.heavy_row;
-    return GSOFA_OK;
+    rc = autotune_impl(ctx, mats, 1, opts);
+    if (rc == GSOFA_OK) ctx->tuned[key] = *opts;
+    return rc;
+}
+
+int gsofa_autotune_batch(gsofa_ctx* ctx, const gsofa_matrix* const* mats, int32_t count,
+                         gsofa_opts* opts) {
+    if (!ctx || !opts || count < 0 || (count > 0 && !mats)) return GSOFA_ERR_ARG;
+    for (int32_t i = 0; i < count; i++)
+        if (!mats[i] || mats[i]->ctx != ctx) return GSOFA_ERR_ARG;
+    std::lock_guard<std::recursive_mutex> g(ctx->mu);
+    int rc = validate_opts(ctx, opts);
+    if (rc) return rc;
+    bool any = false;
+    for (int32_t i = 0; i < count; i++) any |= mats[i]->n > 0;
+    if (!any) return GSOFA_OK;
+    return autotune_impl(ctx, mats, count, opts);
 }
 
 int gsofa_factor_symbolic(gsofa_ctx* ctx, const gsofa_matrix* mat, const gsofa_opts* opts,

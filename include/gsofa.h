@@ -128,6 +128,12 @@ int gsofa_factor_symbolic(gsofa_ctx* ctx, const gsofa_matrix* mat, const gsofa_o
  * similar matrices return at once.  Replaces the reference's fixed sizing
  * (Compute_Src_group, :1031-1048; SPO :1101-1119, :1465-1507). */
 int gsofa_autotune(gsofa_ctx* ctx, const gsofa_matrix* mat, gsofa_opts* opts);
+/* The same search for a batch: each candidate is timed as one persistent
+ * launch over all `count` matrices (what gsofa_factor_batch and
+ * gsofa_batch_create run), so the shape suits the mix rather than its
+ * largest member.  Not cached. */
+int gsofa_autotune_batch(gsofa_ctx* ctx, const gsofa_matrix* const* mats, int32_t count,
+                         gsofa_opts* opts);
 /* Many matrices of uneven size in one persistent launch; results[i] is the
  * result of mats[i] (identical to factoring it alone). */
 int gsofa_factor_batch(gsofa_ctx* ctx, const gsofa_matrix* const* mats, int32_t count,

@@ -293,7 +293,7 @@ def test_autotune_picks_valid_shapes_with_same_results(ctx):
     m = ctx.load_rowptr(rp, col)
     tuned = ctx.autotune(m)
     assert tuned["threads_per_source"] in (128, 256, 512, 1024)
-    assert tuned["chunk_sources"] > 0 and tuned["cached_closures"] in (1, 2, 4, 8, 16, 32)
+    assert tuned["chunk_sources"] > 0 and tuned["cached_closures"] in (1, 2, 4, 8, 16, 32, 64)
     assert ctx.autotune(m) == tuned  # cached for the size class
     a = ctx.factor(m, l_row_stats=True)
     b = ctx.factor(m, l_row_stats=True, **tuned)
@@ -304,6 +304,26 @@ def test_autotune_picks_valid_shapes_with_same_results(ctx):
     a.close()
     b.close()
     m.close()
+
+
+def test_autotune_batch_shapes_give_the_same_results(ctx):
+    from gsofatpds_b200 import gen
+    mats_np = gen.batch_mix(12, nmin=1000, nmax=8000, seed=11)
+    mats = [ctx.load_rowptr(rp, col) for (_, rp, col) in mats_np]
+    tuned = ctx.autotune_batch(mats)
+    assert tuned["threads_per_source"] in (128, 256, 512, 1024)
+    assert tuned["cached_closures"] in (1, 2, 4, 8, 16, 32, 64)
+    alone = [ctx.factor(m) for m in mats]
+    batch = ctx.factor_batch(mats, **tuned)
+    for a, b in zip(alone, batch):
+        for x, y in zip(a.row_counts().values(), b.row_counts().values()):
+            np.testing.assert_array_equal(x, y)
+        np.testing.assert_array_equal(a.supernodes()[0], b.supernodes()[0])
+        assert a.counts["fill_count"] == b.counts["fill_count"]
+        a.close()
+        b.close()
+    for m in mats:
+        m.close()
 
 
 def test_batch_equals_alone(ctx):
