@@ -36,6 +36,8 @@ WORKLOADS = {
     "circuit_like_100k": "circuit-like n=100000 ~0.89M nnz (profiling size), mss 128",
     "batch512": "512 matrices, n log-uniform [2000, 60000]: 2D 5-point ND grids and random-banded "
                 "unsymmetric (bandwidth 4-32, 1-4 uniform off-band entries/row), mss 128",
+    "ingest": "circuit-like n=659033 ~5.84M nnz loaded from the reference's ASCII .dat files, from a "
+              "binary CSR file and from host memory (upload, padded CSR of A and A^T, checks)",
     "serve": "Poisson request stream, n log-uniform [1000, 1000000], 5-27 nnz/row: 2D 5/9-point and "
              "3D 7/27-point ND grids, random-banded unsymmetric (n capped), 40 GB budget, mss 128",
 }
@@ -243,6 +245,51 @@ def run_batch(args, local):
     ctx.close()
 
 
+def run_ingest(args, local):
+    """Input pipeline: the same matrix loaded onto the device from the
+    reference's three ASCII files (parse + build), from one binary CSR file
+    and from host arrays; each timed end to end on the host clock, median of
+    the steps."""
+    import tempfile
+    import torch
+    from gsofatpds_b200 import Context, convert_dat, gen
+    torch.cuda.set_device(local)
+    n, rp, col = gen.circuit_like()
+    with tempfile.TemporaryDirectory() as d:
+        gen.write_dat(os.path.join(d, ""), n, rp, col)
+        paths = [os.path.join(d, "%s_%d.dat" % (k, n)) for k in ("colbeg", "colend", "csr")]
+        binp = os.path.join(d, "m.gsofacsr")
+        t0 = time.perf_counter()
+        convert_dat(*paths, binp)
+        convert_ms = (time.perf_counter() - t0) * 1e3
+        dat_bytes = sum(os.path.getsize(p) for p in paths)
+        bin_bytes = os.path.getsize(binp)
+        with Context(local) as ctx:
+            loaders = {"ascii": lambda: ctx.load_files(*paths),
+                       "binary": lambda: ctx.load_binary(binp),
+                       "memory": lambda: ctx.load_rowptr(rp, col)}
+            res = {}
+            for name, fn in loaders.items():
+                for _ in range(args.warmup):
+                    fn().close()
+                ts = []
+                for _ in range(args.steps):
+                    t0 = time.perf_counter()
+                    m = fn()
+                    ts.append((time.perf_counter() - t0) * 1e3)
+                    m.close()
+                res[name] = float(np.median(ts))
+    line = {"metric": "ingest_ms", "value": res["binary"], "unit": "ms", "n_gpus": 1,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": res["binary"],
+            "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "int32",
+            "data": "synthetic", "config": {"workload": WORKLOADS["ingest"], "n": n,
+                                            "nnz": int(col.shape[0])},
+            "ascii_ms": res["ascii"], "binary_ms": res["binary"], "memory_ms": res["memory"],
+            "convert_ms": convert_ms, "dat_bytes": dat_bytes, "binary_bytes": bin_bytes,
+            "speedup_binary_vs_ascii": res["ascii"] / res["binary"]}
+    print(json.dumps(line), flush=True)
+
+
 def _pct(xs, q):
     return float(np.percentile(np.asarray(xs, dtype=np.float64), q)) if len(xs) else None
 
@@ -371,6 +418,9 @@ def main():
         return
     if args.workload == "serve":
         run_serve(args, local)
+        return
+    if args.workload == "ingest":
+        run_ingest(args, local)
         return
 
     import torch

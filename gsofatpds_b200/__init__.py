@@ -5,8 +5,9 @@ include/gsofa.h); this package is its Python host interface plus the seeded
 input generators.  Importing works without a GPU; the first call that needs
 the library loads it and raises if it is missing.
 """
-from .api import Batch, Context, GsofaError, Matrix, Result, Server, symbfact_min_id  # noqa: F401
+from .api import (Batch, Context, GsofaError, Matrix, Result, Server, convert_dat,  # noqa: F401
+                  read_binary, symbfact_min_id, write_binary)
 from . import gen  # noqa: F401
 
 __all__ = ["Batch", "Context", "GsofaError", "Matrix", "Result", "Server", "symbfact_min_id",
-           "gen"]
+           "write_binary", "read_binary", "convert_dat", "gen"]

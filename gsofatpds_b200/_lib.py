@@ -41,6 +41,8 @@ EXPORTS = [
     "gsofa_batch_destroy", "gsofa_server_create", "gsofa_server_submit", "gsofa_server_poll",
     "gsofa_server_wait", "gsofa_server_ticket_info", "gsofa_server_get_stats",
     "gsofa_server_destroy", "gsofa_server_last_error", "gsofa_autotune_batch",
+    "gsofa_write_csr_binary", "gsofa_read_csr_binary", "gsofa_convert_dat_to_binary",
+    "gsofa_load_csr_binary",
 ]
 
 
@@ -119,6 +121,12 @@ def load():
         "gsofa_result_destroy": [vp],
         "gsofa_autotune": [vp, vp, ctypes.POINTER(Opts)],
         "gsofa_autotune_batch": [vp, ctypes.POINTER(vp), i32, ctypes.POINTER(Opts)],
+        "gsofa_write_csr_binary": [ctypes.c_char_p, i32, i64, vp, vp, vp],
+        "gsofa_read_csr_binary": [ctypes.c_char_p, ctypes.POINTER(i32), ctypes.POINTER(i64), vp, vp,
+                                  vp],
+        "gsofa_convert_dat_to_binary": [ctypes.c_char_p, ctypes.c_char_p, ctypes.c_char_p,
+                                        ctypes.c_char_p],
+        "gsofa_load_csr_binary": [vp, ctypes.c_char_p, ctypes.POINTER(vp)],
         "gsofa_batch_create": [vp, ctypes.POINTER(vp), i32, ctypes.POINTER(Opts), ctypes.POINTER(vp)],
         "gsofa_batch_run": [vp],
         "gsofa_batch_result": [vp, i32, ctypes.POINTER(vp)],

@@ -10,12 +10,14 @@ callers that keep matrices device-resident.  Errors raise ``GsofaError``
 carrying the library's status code; nothing here falls back to the CPU.
 """
 import ctypes
+import os
 
 import numpy as np
 
 from . import _lib as C
 
-__all__ = ["GsofaError", "Context", "Matrix", "Result", "Batch", "Server", "symbfact_min_id"]
+__all__ = ["GsofaError", "Context", "Matrix", "Result", "Batch", "Server", "symbfact_min_id",
+           "write_binary", "read_binary", "convert_dat"]
 
 
 class GsofaError(RuntimeError):
@@ -75,6 +77,13 @@ class Context:
     def load_rowptr(self, rowptr, col):
         rowptr = np.ascontiguousarray(rowptr, dtype=np.int32)
         return self.load_csr(rowptr[:-1], rowptr[1:], col)
+
+    def load_binary(self, path):
+        """A matrix from a binary CSR file (see write_binary)."""
+        h = ctypes.c_void_p()
+        self._check(self._L.gsofa_load_csr_binary(self._h, os.fsencode(path), ctypes.byref(h)),
+                    "load_csr_binary")
+        return Matrix(self, h)
 
     def load_files(self, beg_file, end_file, csr_file):
         h = ctypes.c_void_p()
@@ -355,6 +364,43 @@ class Result:
             if self._owned:
                 self.ctx._L.gsofa_result_destroy(self._h)
             self._h = None
+
+
+def write_binary(path, row_begin, row_end, col):
+    """Binary CSR file (row v = col[row_begin[v]:row_end[v]]); no GPU needed."""
+    beg = np.ascontiguousarray(row_begin, dtype=np.int32)
+    end = np.ascontiguousarray(row_end, dtype=np.int32)
+    c = np.ascontiguousarray(col, dtype=np.int32)
+    rc = C.load().gsofa_write_csr_binary(os.fsencode(path), beg.shape[0], c.shape[0], _ptr(beg),
+                                         _ptr(end), _ptr(c))
+    if rc != C.OK:
+        raise GsofaError(rc, "write_csr_binary %s" % path)
+
+
+def read_binary(path):
+    """(row_begin, row_end, col) of a binary CSR file; no GPU needed."""
+    L = C.load()
+    n, nnz = ctypes.c_int32(), ctypes.c_int64()
+    rc = L.gsofa_read_csr_binary(os.fsencode(path), ctypes.byref(n), ctypes.byref(nnz), None, None,
+                                 None)
+    if rc != C.OK:
+        raise GsofaError(rc, "read_csr_binary %s" % path)
+    beg = np.zeros(n.value, np.int32)
+    end = np.zeros(n.value, np.int32)
+    col = np.zeros(max(nnz.value, 1), np.int32)
+    rc = L.gsofa_read_csr_binary(os.fsencode(path), ctypes.byref(n), ctypes.byref(nnz), _ptr(beg),
+                                 _ptr(end), _ptr(col))
+    if rc != C.OK:
+        raise GsofaError(rc, "read_csr_binary %s" % path)
+    return beg, end, col[:nnz.value]
+
+
+def convert_dat(beg_file, end_file, csr_file, out_path):
+    """The reference's three ASCII files into one binary CSR file."""
+    rc = C.load().gsofa_convert_dat_to_binary(os.fsencode(beg_file), os.fsencode(end_file),
+                                              os.fsencode(csr_file), os.fsencode(out_path))
+    if rc != C.OK:
+        raise GsofaError(rc, "convert_dat_to_binary -> %s" % out_path)
 
 
 def symbfact_min_id(argv, rank=0):

@@ -477,6 +477,39 @@ int64_t parse_ints(const std::string& s, size_t* pos, int64_t count, int32_t* ou
     return i;
 }
 
+// The reference's three ASCII files (csr = "E N" then E column ids, beg /
+// end = n ids each) into host arrays.  ctx may be null (no message kept).
+int parse_dat_files(gsofa_ctx* ctx, const char* beg_file, const char* end_file,
+                    const char* csr_file, int32_t* n_out, int64_t* nnz_out,
+                    std::vector<int32_t>* beg, std::vector<int32_t>* end,
+                    std::vector<int32_t>* col) {
+    std::string sc, sb, se;
+    if (read_file(csr_file, &sc)) return set_err(ctx, GSOFA_ERR_IO, "cannot read %s", csr_file);
+    size_t pos = 0;
+    bool bad = false;
+    int32_t hdr[2];
+    if (parse_ints(sc, &pos, 2, hdr, &bad) != 2 || bad || hdr[0] < 0 || hdr[1] < 0)
+        return set_err(ctx, GSOFA_ERR_IO, "%s: bad header (expected E N)", csr_file);
+    const int64_t E = hdr[0];
+    const int32_t n = hdr[1];
+    col->assign((size_t)std::max<int64_t>(E, 1), 0);
+    beg->assign((size_t)n + 1, 0);
+    end->assign((size_t)n + 1, 0);
+    if (parse_ints(sc, &pos, E, col->data(), &bad) != E || bad)
+        return set_err(ctx, GSOFA_ERR_IO, "%s: expected %lld column ids", csr_file, (long long)E);
+    if (read_file(beg_file, &sb)) return set_err(ctx, GSOFA_ERR_IO, "cannot read %s", beg_file);
+    if (read_file(end_file, &se)) return set_err(ctx, GSOFA_ERR_IO, "cannot read %s", end_file);
+    pos = 0;
+    if (parse_ints(sb, &pos, n, beg->data(), &bad) != n || bad)
+        return set_err(ctx, GSOFA_ERR_IO, "%s: expected %d row starts", beg_file, n);
+    pos = 0;
+    if (parse_ints(se, &pos, n, end->data(), &bad) != n || bad)
+        return set_err(ctx, GSOFA_ERR_IO, "%s: expected %d row ends", end_file, n);
+    *n_out = n;
+    *nnz_out = E;
+    return GSOFA_OK;
+}
+
 }  // namespace host
 }  // namespace gsofa
 
@@ -773,26 +806,11 @@ int gsofa_load_csr(gsofa_ctx* ctx, int32_t n, int64_t nnz, const int32_t* row_be
 int gsofa_load_csr_files(gsofa_ctx* ctx, const char* beg_file, const char* end_file,
                          const char* csr_file, gsofa_matrix** out) {
     if (!ctx || !out || !beg_file || !end_file || !csr_file) return GSOFA_ERR_ARG;
-    std::string sc, sb, se;
-    if (read_file(csr_file, &sc)) return set_err(ctx, GSOFA_ERR_IO, "cannot read %s", csr_file);
-    size_t pos = 0;
-    bool bad = false;
-    int32_t hdr[2];
-    if (parse_ints(sc, &pos, 2, hdr, &bad) != 2 || bad || hdr[0] < 0 || hdr[1] < 0)
-        return set_err(ctx, GSOFA_ERR_IO, "%s: bad header (expected E N)", csr_file);
-    const int64_t E = hdr[0];
-    const int32_t n = hdr[1];
-    std::vector<int32_t> col((size_t)std::max<int64_t>(E, 1)), beg((size_t)n + 1), end((size_t)n + 1);
-    if (parse_ints(sc, &pos, E, col.data(), &bad) != E || bad)
-        return set_err(ctx, GSOFA_ERR_IO, "%s: expected %lld column ids", csr_file, (long long)E);
-    if (read_file(beg_file, &sb)) return set_err(ctx, GSOFA_ERR_IO, "cannot read %s", beg_file);
-    if (read_file(end_file, &se)) return set_err(ctx, GSOFA_ERR_IO, "cannot read %s", end_file);
-    pos = 0;
-    if (parse_ints(sb, &pos, n, beg.data(), &bad) != n || bad)
-        return set_err(ctx, GSOFA_ERR_IO, "%s: expected %d row starts", beg_file, n);
-    pos = 0;
-    if (parse_ints(se, &pos, n, end.data(), &bad) != n || bad)
-        return set_err(ctx, GSOFA_ERR_IO, "%s: expected %d row ends", end_file, n);
+    int32_t n = 0;
+    int64_t E = 0;
+    std::vector<int32_t> beg, end, col;
+    int rc = parse_dat_files(ctx, beg_file, end_file, csr_file, &n, &E, &beg, &end, &col);
+    if (rc) return rc;
     return gsofa_load_csr(ctx, n, E, beg.data(), end.data(), col.data(), out);
 }
 

@@ -104,6 +104,10 @@ namespace gsofa {
 namespace host {
 
 int set_err(gsofa_ctx* ctx, int status, const char* fmt, ...);
+// The reference's three ASCII files into host arrays (ctx may be null).
+int parse_dat_files(gsofa_ctx* ctx, const char* beg_file, const char* end_file,
+                    const char* csr_file, int32_t* n, int64_t* nnz, std::vector<int32_t>* beg,
+                    std::vector<int32_t>* end, std::vector<int32_t>* col);
 int cuda_fail(gsofa_ctx* ctx, cudaError_t e, const char* where);
 // Pool allocation with budget accounting, ordered on `stream`; the caller
 // holds ctx->mu.

@@ -113,6 +113,20 @@ int gsofa_load_csr(gsofa_ctx* ctx, int32_t n, int64_t nnz, const int32_t* row_be
  * beg / end = n ids each. */
 int gsofa_load_csr_files(gsofa_ctx* ctx, const char* beg_file, const char* end_file,
                          const char* csr_file, gsofa_matrix** out);
+/* Binary CSR files: the parsed form of the three ASCII files, read at disk
+ * speed instead of being parsed again (the reference reads the ASCII files
+ * with fscanf on every run, :2567-2616).  Little-endian: "GSOFACSR", version,
+ * n, nnz, a payload checksum, then beg[n], end[n], col[nnz] as int32 exactly
+ * as in the .dat files.  Writing and reading need no GPU; a truncated or
+ * corrupted file is GSOFA_ERR_IO. */
+int gsofa_write_csr_binary(const char* path, int32_t n, int64_t nnz, const int32_t* row_begin,
+                           const int32_t* row_end, const int32_t* col);
+/* With all three arrays NULL, only *n and *nnz are returned (size query). */
+int gsofa_read_csr_binary(const char* path, int32_t* n, int64_t* nnz, int32_t* row_begin,
+                          int32_t* row_end, int32_t* col);
+int gsofa_convert_dat_to_binary(const char* beg_file, const char* end_file, const char* csr_file,
+                                const char* out_path);
+int gsofa_load_csr_binary(gsofa_ctx* ctx, const char* path, gsofa_matrix** out);
 int gsofa_matrix_info(const gsofa_matrix* mat, int32_t* n, int64_t* nnz);
 int gsofa_matrix_destroy(gsofa_matrix* mat);
 
