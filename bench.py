@@ -38,6 +38,8 @@ WORKLOADS = {
                 "unsymmetric (bandwidth 4-32, 1-4 uniform off-band entries/row), mss 128",
     "ingest": "circuit-like n=659033 ~5.84M nnz loaded from the reference's ASCII .dat files, from a "
               "binary CSR file and from host memory (upload, padded CSR of A and A^T, checks)",
+    "handoff": "supernodal block form (gsofa_result_supernodal) of the n=20000 random matrix and the "
+               "64^3 ND grid, from their materialised patterns, mss 128",
     "serve": "Poisson request stream, n log-uniform [1000, 1000000], 5-27 nnz/row: 2D 5/9-point and "
              "3D 7/27-point ND grids, random-banded unsymmetric (n capped), 40 GB budget, mss 128",
 }
@@ -290,6 +292,45 @@ def run_ingest(args, local):
     print(json.dumps(line), flush=True)
 
 
+def run_handoff(args, local):
+    """Symbolic-to-numeric handoff: factor with the pattern materialised,
+    then time building the supernodal block form on the device (first call
+    of gsofa_result_supernodal, read-back of the arrays included)."""
+    import ctypes
+    import torch
+    from gsofatpds_b200 import Context, gen
+    torch.cuda.set_device(local)
+    out = {}
+    with Context(local) as ctx:
+        for name, (n, rp, col) in [("random_extra_20k", gen.random_extra(20000, 3, seed=1)),
+                                   ("grid3d_64", gen.grid_nd((64, 64, 64), "7"))]:
+            m = ctx.load_rowptr(rp, col)
+            ts, pairs = [], 0
+            for it in range(args.warmup + args.steps):
+                r = ctx.factor(m, pattern=True)
+                nb, nl, nu = ctypes.c_int64(), ctypes.c_int64(), ctypes.c_int64()
+                t0 = time.perf_counter()
+                rc = ctx._L.gsofa_result_supernodal(r._h, ctypes.byref(nb), ctypes.byref(nl),
+                                                    ctypes.byref(nu), None, None, None, None, None)
+                ms = (time.perf_counter() - t0) * 1e3
+                assert rc == 0
+                pairs = r.counts["nnz_l"] + r.counts["nnz_u"]
+                if it >= args.warmup:
+                    ts.append(ms)
+                out[name] = dict(build_ms=float(np.median(ts)) if ts else None, blocks=nb.value,
+                                 l_rows=nl.value, u_cols=nu.value, pattern_entries=pairs)
+                r.close()
+            m.close()
+            out[name]["pattern_entries_per_s"] = out[name]["pattern_entries"] / (
+                out[name]["build_ms"] / 1e3)
+    tot = sum(v["build_ms"] for v in out.values())
+    line = {"metric": "handoff_ms", "value": tot, "unit": "ms", "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": tot, "higher_is_better": False,
+            "scaling": "weak", "vs_baseline": None, "dtype": "int32", "data": "synthetic",
+            "config": {"workload": WORKLOADS["handoff"]}, "cases": out}
+    print(json.dumps(line), flush=True)
+
+
 def _pct(xs, q):
     return float(np.percentile(np.asarray(xs, dtype=np.float64), q)) if len(xs) else None
 
@@ -421,6 +462,9 @@ def main():
         return
     if args.workload == "ingest":
         run_ingest(args, local)
+        return
+    if args.workload == "handoff":
+        run_handoff(args, local)
         return
 
     import torch

@@ -42,7 +42,7 @@ EXPORTS = [
     "gsofa_server_wait", "gsofa_server_ticket_info", "gsofa_server_get_stats",
     "gsofa_server_destroy", "gsofa_server_last_error", "gsofa_autotune_batch",
     "gsofa_write_csr_binary", "gsofa_read_csr_binary", "gsofa_convert_dat_to_binary",
-    "gsofa_load_csr_binary",
+    "gsofa_load_csr_binary", "gsofa_result_supernodal",
 ]
 
 
@@ -127,6 +127,8 @@ def load():
         "gsofa_convert_dat_to_binary": [ctypes.c_char_p, ctypes.c_char_p, ctypes.c_char_p,
                                         ctypes.c_char_p],
         "gsofa_load_csr_binary": [vp, ctypes.c_char_p, ctypes.POINTER(vp)],
+        "gsofa_result_supernodal": [vp, ctypes.POINTER(i64), ctypes.POINTER(i64), ctypes.POINTER(i64),
+                                    vp, vp, vp, vp, vp],
         "gsofa_batch_create": [vp, ctypes.POINTER(vp), i32, ctypes.POINTER(Opts), ctypes.POINTER(vp)],
         "gsofa_batch_run": [vp],
         "gsofa_batch_result": [vp, i32, ctypes.POINTER(vp)],

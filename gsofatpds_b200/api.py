@@ -351,6 +351,23 @@ class Result:
         self.ctx._check(fn(self._h, _ptr(ptr), _ptr(ids), ids.shape[0]), "pattern")
         return ptr, ids[:ptr[-1]]
 
+    def supernodal(self):
+        """Supernodal block form: block_start (nblocks + 1), and per block the
+        sorted off-block L rows (lptr, lrows) and U columns (uptr, ucols)."""
+        nb, nl, nu = ctypes.c_int64(), ctypes.c_int64(), ctypes.c_int64()
+        f = self.ctx._L.gsofa_result_supernodal
+        self.ctx._check(f(self._h, ctypes.byref(nb), ctypes.byref(nl), ctypes.byref(nu), None, None,
+                          None, None, None), "supernodal")
+        start = np.zeros(nb.value + 1, np.int32)
+        lptr = np.zeros(nb.value + 1, np.int64)
+        uptr = np.zeros(nb.value + 1, np.int64)
+        lrows = np.zeros(max(nl.value, 1), np.int32)
+        ucols = np.zeros(max(nu.value, 1), np.int32)
+        self.ctx._check(f(self._h, None, None, None, _ptr(start), _ptr(lptr), _ptr(lrows), _ptr(uptr),
+                          _ptr(ucols)), "supernodal")
+        return dict(block_start=start, lptr=lptr, lrows=lrows[:nl.value], uptr=uptr,
+                    ucols=ucols[:nu.value])
+
     def pattern_u(self):
         """U by rows: (rowptr[n+1], sorted column ids)."""
         return self._pattern(self.ctx._L.gsofa_result_pattern_u)

@@ -167,6 +167,7 @@ void result_free(gsofa_result* r) {
         std::lock_guard<std::recursive_mutex> g(r->ctx->mu);
         dev_free(r->ctx, r->arena, r->bytes);
         dev_free(r->ctx, r->parena, r->pbytes);
+        supernodal_free(r);
     }
     delete r;
 }

@@ -81,6 +81,14 @@ struct gsofa_result {
     int32_t* ucols = nullptr;
     int64_t* lptr = nullptr;
     int32_t* lrows = nullptr;
+    // supernodal block form (gsofa_result_supernodal), built on first request
+    bool sn_built = false;
+    long long sn_nblocks = 0, sn_nl = 0, sn_nu = 0;
+    int32_t* sn_start = nullptr;
+    int64_t* sn_lptr = nullptr;
+    int32_t* sn_lrows = nullptr;
+    int64_t* sn_uptr = nullptr;
+    int32_t* sn_ucols = nullptr;
     gsofa_counts counts{};
     bool batch_owned = false;  // lives inside a gsofa_batch: not destroyed alone
 };
@@ -120,6 +128,7 @@ int default_block(int32_t nmax, int smem_per_sm);
 int result_alloc_on(gsofa_ctx* ctx, int32_t n, uint32_t flags, int32_t mss, cudaStream_t stream,
                     gsofa_result** out);
 void result_free(gsofa_result* r);
+void supernodal_free(gsofa_result* r);  // caller holds ctx->mu
 MatDesc make_desc(const gsofa_matrix* m, const gsofa_result* r, long long base);
 // Validates the row intervals on the host, then queues the upload and the
 // padded-CSR build of A and A^T on `stream` without waiting.  Column ids

@@ -214,6 +214,23 @@ int gsofa_result_lmask(const gsofa_result* res, uint32_t* mask4n);
  * get ptr only. */
 int gsofa_result_pattern_u(const gsofa_result* res, int64_t* ptr, int32_t* cols, int64_t cap);
 int gsofa_result_pattern_l(const gsofa_result* res, int64_t* ptr, int32_t* rows, int64_t cap);
+/* The symbolic-to-numeric handoff (needs GSOFA_PATTERN and GSOFA_SUPERNODES):
+ * L and U in supernodal block form, what a supernodal numeric LU allocates
+ * from.  Block k is the run of columns [block_start[k], block_start[k+1]),
+ * a new block starting at every row with a non-zero supernode flag.  With
+ * l = block_start[k+1]:
+ *   lrows[lptr[k] .. lptr[k+1])  sorted rows r >= l with L(r, c) != 0 for
+ *                                some column c of the block;
+ *   ucols[uptr[k] .. uptr[k+1])  sorted columns c >= l with U(r, c) != 0 for
+ *                                some row r of the block;
+ * the diagonal block is dense and implicit.  Call with NULL arrays to get
+ * the sizes (*nblocks, *nl, *nu); buffers then need nblocks + 1, nl and nu
+ * entries.  Built on the device on the first call and kept with the result.
+ * No counterpart in the reference, which stops at counts (its consumer,
+ * SuperLU_DIST, recomputes the structure). */
+int gsofa_result_supernodal(const gsofa_result* res, int64_t* nblocks, int64_t* nl, int64_t* nu,
+                            int32_t* block_start, int64_t* lptr, int32_t* lrows, int64_t* uptr,
+                            int32_t* ucols);
 int gsofa_result_destroy(gsofa_result* res);
 
 /* ---- serving: a request loop with continuous batching ------------------------ */

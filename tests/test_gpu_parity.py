@@ -508,3 +508,54 @@ def test_symmetric_pattern_shortcut(ctx):
     check_full(res, r, rt)
     res.close()
     m.close()
+
+
+def _supernodal_reference(n, r, flags):
+    """The supernodal block form from the oracle's own patterns: L rows
+    (transposed to columns) and U rows, blocks from the oracle's flags."""
+    starts = [int(x) for x in np.nonzero(flags)[0]] + [n]
+    lcols = [[] for _ in range(n)]
+    for s in range(n):
+        for c in r["Lcols"][r["Lptr"][s]:r["Lptr"][s + 1]]:
+            lcols[int(c)].append(s)
+    out = dict(block_start=np.array(starts, np.int32), lptr=[0], lrows=[], uptr=[0], ucols=[])
+    for k in range(len(starts) - 1):
+        f, l = starts[k], starts[k + 1]
+        rows, cols = set(), set()
+        for c in range(f, l):
+            rows.update(x for x in lcols[c] if x >= l)
+            cols.update(int(x) for x in r["Ucols"][r["Uptr"][c]:r["Uptr"][c + 1]] if x >= l)
+        out["lrows"] += sorted(rows)
+        out["ucols"] += sorted(cols)
+        out["lptr"].append(len(out["lrows"]))
+        out["uptr"].append(len(out["ucols"]))
+    return out
+
+
+@pytest.mark.parametrize("which", ["bc", "grid", "random"])
+def test_supernodal_handoff_matches_oracle(ctx, which):
+    """gsofa_result_supernodal against a restatement from the oracle's
+    patterns and supernode partition."""
+    from gsofatpds_b200 import gen
+    if which == "bc":
+        z = load_bc()
+        beg, end, col = z["beg"], z["end"], z["col"]
+    elif which == "grid":
+        _, rp, col = gen.grid_nd((12, 12, 12), "7")
+        beg, end = rp[:-1], rp[1:]
+    else:
+        _, rp, col = gen.random_banded(3000, bw=6, extra=2, seed=9)
+        beg, end = rp[:-1], rp[1:]
+    n = beg.shape[0]
+    r = O.rows(beg, end, col, pattern=True)
+    nsup, flags = O.supernodes(r["nzU_ref"], r["lback"], 128)
+    ref = _supernodal_reference(n, r, flags)
+    m = ctx.load_csr(beg, end, col)
+    res = ctx.factor(m, pattern=True)
+    got = res.supernodal()
+    np.testing.assert_array_equal(got["block_start"], ref["block_start"])
+    for k in ("lptr", "lrows", "uptr", "ucols"):
+        np.testing.assert_array_equal(got[k], np.array(ref[k]), err_msg=k)
+    assert res.supernodal()["lrows"].shape == got["lrows"].shape  # cached, same answer
+    res.close()
+    m.close()
