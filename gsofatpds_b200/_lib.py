@@ -42,7 +42,7 @@ EXPORTS = [
     "gsofa_server_wait", "gsofa_server_ticket_info", "gsofa_server_get_stats",
     "gsofa_server_destroy", "gsofa_server_last_error", "gsofa_autotune_batch",
     "gsofa_write_csr_binary", "gsofa_read_csr_binary", "gsofa_convert_dat_to_binary",
-    "gsofa_load_csr_binary", "gsofa_result_supernodal",
+    "gsofa_load_csr_binary", "gsofa_result_supernodal", "gsofa_order_nd", "gsofa_matrix_permute",
 ]
 
 
@@ -67,6 +67,12 @@ class Counts(ctypes.Structure):
                 ("n_supernodes", ctypes.c_int64), ("edges_alg", ctypes.c_uint64),
                 ("vertices_alg", ctypes.c_uint64), ("edges_traversed", ctypes.c_uint64),
                 ("ms_device", ctypes.c_double), ("ms_traverse", ctypes.c_double)]
+
+
+class OrderStats(ctypes.Structure):
+    _fields_ = [("rounds", ctypes.c_int32), ("splits", ctypes.c_int32),
+                ("separator_vertices", ctypes.c_int64), ("max_separator", ctypes.c_int32),
+                ("reserved", ctypes.c_int32), ("ms", ctypes.c_double)]
 
 
 class TicketInfo(ctypes.Structure):
@@ -129,6 +135,8 @@ def load():
         "gsofa_load_csr_binary": [vp, ctypes.c_char_p, ctypes.POINTER(vp)],
         "gsofa_result_supernodal": [vp, ctypes.POINTER(i64), ctypes.POINTER(i64), ctypes.POINTER(i64),
                                     vp, vp, vp, vp, vp],
+        "gsofa_order_nd": [vp, vp, i32, i32, vp, ctypes.POINTER(OrderStats)],
+        "gsofa_matrix_permute": [vp, vp, vp, ctypes.POINTER(vp)],
         "gsofa_batch_create": [vp, ctypes.POINTER(vp), i32, ctypes.POINTER(Opts), ctypes.POINTER(vp)],
         "gsofa_batch_run": [vp],
         "gsofa_batch_result": [vp, i32, ctypes.POINTER(vp)],

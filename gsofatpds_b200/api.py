@@ -128,6 +128,29 @@ class Context:
         return dict(threads_per_source=o.threads_per_source, chunk_sources=o.chunk_sources,
                     cached_closures=o.cached_closures, heavy_row=o.heavy_row)
 
+    def order_nd(self, mat, leaf_size=0, max_rounds=0):
+        """Fill-reducing ordering of A + A^T by level-set nested dissection,
+        computed on the device.  Returns (perm, stats): new index k holds
+        old index perm[k]."""
+        n = mat.n
+        perm = np.zeros(max(n, 1), np.int32)
+        st = C.OrderStats()
+        self._check(self._L.gsofa_order_nd(self._h, mat.handle, int(leaf_size), int(max_rounds),
+                                           _ptr(perm), ctypes.byref(st)), "order_nd")
+        stats = {f: getattr(st, f) for f, _ in C.OrderStats._fields_ if f != "reserved"}
+        return perm[:n], stats
+
+    def permute(self, mat, perm):
+        """P A P^T on the device: row k is row perm[k] of `mat`, columns renamed."""
+        p = np.ascontiguousarray(perm, dtype=np.int32)
+        if p.shape[0] != mat.n:
+            raise GsofaError(C.ERR_ARG, "perm has %d entries, the matrix %d rows" %
+                             (p.shape[0], mat.n))
+        h = ctypes.c_void_p()
+        self._check(self._L.gsofa_matrix_permute(self._h, mat.handle, _ptr(p), ctypes.byref(h)),
+                    "matrix_permute")
+        return Matrix(self, h)
+
     def factor(self, mat, **kw):
         o = self.opts(**kw)
         h = ctypes.c_void_p()

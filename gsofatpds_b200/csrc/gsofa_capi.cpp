@@ -568,19 +568,51 @@ int gsofa::host::ingest_csr(gsofa_ctx* ctx, cudaStream_t stream, int32_t* dstatu
         rp[(size_t)v + 1] = (int32_t)(acc | (pd - d));
     }
     const int64_t padded = acc;
+    int nplanes = 0;
+    while (nplanes < 32 && (maxd >> nplanes) != 0) nplanes++;
+    gsofa_matrix* m = nullptr;
+    int rc = matrix_alloc(ctx, stream, n, real, padded, nplanes, &m);
+    if (rc) return rc;
+    // staging: the raw input (row starts, column ids)
+    const size_t N1 = (size_t)n + 1;
+    const size_t Nin = (size_t)std::max<int64_t>(nnz, 1);
+    const size_t stage = align256(4 * N1) + align256(4 * Nin);
+    void* sblk = nullptr;
+    rc = dev_alloc_on(ctx, stage, &sblk, stream);
+    if (rc) { matrix_free_on(m, stream); return rc; }
+    int32_t* dbeg = reinterpret_cast<int32_t*>(sblk);
+    int32_t* dcol_in = reinterpret_cast<int32_t*>(reinterpret_cast<char*>(sblk) + align256(4 * N1));
+    cudaError_t e = cudaMemcpyAsync(m->rowptr, rp.data(), 4 * N1, cudaMemcpyHostToDevice, stream);
+    if (e == cudaSuccess && n > 0)
+        e = cudaMemcpyAsync(dbeg, row_begin, 4 * (size_t)n, cudaMemcpyHostToDevice, stream);
+    if (e == cudaSuccess && nnz > 0)
+        e = cudaMemcpyAsync(dcol_in, col, 4 * (size_t)nnz, cudaMemcpyHostToDevice, stream);
+    if (e != cudaSuccess) {
+        dev_free_on(ctx, sblk, stage, stream);
+        matrix_free_on(m, stream);
+        return cuda_fail(ctx, e, "ingest upload");
+    }
+    rc = matrix_build(ctx, stream, dstatus, m, nnz, dbeg, dcol_in,
+                      maxd <= kSymmetryCheckMaxRow ? 1 : 0);
+    dev_free_on(ctx, sblk, stage, stream);  // stream-ordered: after the build
+    if (rc) { matrix_free_on(m, stream); return rc; }
+    *out = m;
+    return GSOFA_OK;
+}
 
+int gsofa::host::matrix_alloc(gsofa_ctx* ctx, cudaStream_t stream, int32_t n, int64_t real,
+                              int64_t padded, int nplanes, gsofa_matrix** out) {
+    *out = nullptr;
     gsofa_matrix* m = new (std::nothrow) gsofa_matrix();
     if (!m) return set_err(ctx, GSOFA_ERR_OOM_BUDGET, "host allocation failed");
     m->ctx = ctx;
     m->n = n;
     m->nnz = real;
+    m->nplanes = nplanes;
     const size_t N1 = (size_t)n + 1;
     const size_t PA = (size_t)std::max<int64_t>(padded, 4);
     const size_t PT = (size_t)std::max<int64_t>(real + 3ll * n, 4);  // bound for A^T
     const size_t NW = (size_t)(((int64_t)n + 31) >> 5) + 1;
-    int nplanes = 0;
-    while (nplanes < 32 && (maxd >> nplanes) != 0) nplanes++;
-    m->nplanes = nplanes;
     size_t total = align256(4 * N1) * 2 + align256(4 * PA) + align256(4 * PT) + align256(4 * NW) +
                    align256(4 * NW * (size_t)std::max(nplanes, 1)) + 256;
     void* blk = nullptr;
@@ -597,20 +629,27 @@ int gsofa::host::ingest_csr(gsofa_ctx* ctx, cudaStream_t stream, int32_t* dstatu
     m->dplanes = reinterpret_cast<uint32_t*>(b + 2 * align256(4 * N1) + align256(4 * PA) +
                                              align256(4 * PT) + align256(4 * NW));
     m->asym = reinterpret_cast<int32_t*>(b + total - 256);
+    *out = m;
+    return GSOFA_OK;
+}
 
-    // staging: raw input (beg, col_in) and the transpose's counters
-    const size_t Nin = (size_t)std::max<int64_t>(nnz, 1);
+void gsofa::host::matrix_free_on(gsofa_matrix* m, cudaStream_t stream) {
+    if (!m) return;
+    dev_free_on(m->ctx, m->rowptr, m->bytes, stream);
+    delete m;
+}
+
+int gsofa::host::matrix_build(gsofa_ctx* ctx, cudaStream_t stream, int32_t* dstatus,
+                              gsofa_matrix* m, int64_t nnz_in, const int32_t* dbeg,
+                              const int32_t* dcol_in, int check_symmetry) {
+    const int32_t n = m->n;
+    const size_t N1 = (size_t)n + 1;
     size_t scan_bytes = canonicalize_scan_bytes(n);
-    size_t stage = align256(4 * N1) + align256(4 * Nin) + align256(4 * N1) * 3 +
-                   align256(scan_bytes) + 256;
+    const size_t stage = align256(4 * N1) * 3 + align256(scan_bytes) + 256;
     void* sblk = nullptr;
-    rc = dev_alloc_on(ctx, stage, &sblk, stream);
-    if (rc) { dev_free_on(ctx, blk, total, stream); delete m; return rc; }
+    int rc = dev_alloc_on(ctx, stage, &sblk, stream);
+    if (rc) return rc;
     char* s = reinterpret_cast<char*>(sblk);
-    int32_t* dbeg = reinterpret_cast<int32_t*>(s);
-    s += align256(4 * N1);
-    int32_t* dcol_in = reinterpret_cast<int32_t*>(s);
-    s += align256(4 * Nin);
     int32_t* tcount = reinterpret_cast<int32_t*>(s);
     s += align256(4 * N1);
     int32_t* tfill = reinterpret_cast<int32_t*>(s);
@@ -618,36 +657,16 @@ int gsofa::host::ingest_csr(gsofa_ctx* ctx, cudaStream_t stream, int32_t* dstatu
     int32_t* tpad = reinterpret_cast<int32_t*>(s);
     s += align256(4 * N1);
     void* scan_tmp = s;
-
     cudaError_t e = cudaSuccess;
-    auto cleanup = [&]() {
-        dev_free_on(ctx, sblk, stage, stream);
-        dev_free_on(ctx, blk, total, stream);
-        delete m;
-    };
-#define CKL(call)                                        \
-    do {                                                 \
-        e = (call);                                      \
-        if (e != cudaSuccess) { cleanup(); return cuda_fail(ctx, e, #call); } \
-    } while (0)
-    CKL(cudaMemcpyAsync(m->rowptr, rp.data(), 4 * N1, cudaMemcpyHostToDevice, stream));
-    if (n > 0) {
-        CKL(cudaMemcpyAsync(dbeg, row_begin, 4 * (size_t)n, cudaMemcpyHostToDevice, stream));
-    } else {
-        CKL(cudaMemsetAsync(m->trowptr, 0, 4, stream));
-    }
-    if (nnz > 0)
-        CKL(cudaMemcpyAsync(dcol_in, col, 4 * (size_t)nnz, cudaMemcpyHostToDevice, stream));
-    CKL(cudaMemsetAsync(tcount, 0, 4 * N1, stream));
-    CKL(cudaMemsetAsync(tfill, 0, 4 * N1, stream));
-    CKL(launch_canonicalize(n, nnz, dbeg, dcol_in, m->rowptr, m->col, tcount, tpad, m->trowptr,
-                            m->tcol, tfill, m->wdeg, m->dplanes, m->nplanes, m->asym,
-                            maxd <= kSymmetryCheckMaxRow ? 1 : 0, scan_tmp, scan_bytes, dstatus,
-                            stream));
-#undef CKL
+    if (n == 0) e = cudaMemsetAsync(m->trowptr, 0, 4, stream);
+    if (e == cudaSuccess) e = cudaMemsetAsync(tcount, 0, 4 * N1, stream);
+    if (e == cudaSuccess) e = cudaMemsetAsync(tfill, 0, 4 * N1, stream);
+    if (e == cudaSuccess)
+        e = launch_canonicalize(n, nnz_in, dbeg, dcol_in, m->rowptr, m->col, tcount, tpad,
+                                m->trowptr, m->tcol, tfill, m->wdeg, m->dplanes, m->nplanes,
+                                m->asym, check_symmetry, scan_tmp, scan_bytes, dstatus, stream);
     dev_free_on(ctx, sblk, stage, stream);  // stream-ordered: after the build
-    *out = m;
-    return GSOFA_OK;
+    return e == cudaSuccess ? GSOFA_OK : cuda_fail(ctx, e, "matrix build");
 }
 
 // ============================================================================

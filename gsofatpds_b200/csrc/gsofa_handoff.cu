@@ -112,24 +112,10 @@ int grid_for(long long items, int threads) {
     return (int)std::max(1ll, std::min(g, 148ll * 32));
 }
 
-struct Scratch {
-    gsofa_ctx* ctx;
-    std::vector<std::pair<void*, size_t>> blocks;
-    void* get(size_t bytes) {
-        void* p = nullptr;
-        if (dev_alloc_on(ctx, std::max<size_t>(bytes, 16), &p, ctx->stream)) return nullptr;
-        blocks.emplace_back(p, std::max<size_t>(bytes, 16));
-        return p;
-    }
-    ~Scratch() {
-        for (auto& b : blocks) dev_free_on(ctx, b.first, b.second, ctx->stream);
-    }
-};
-
 // Unique sorted (block, index) pairs of one side; returns their count and
 // leaves ptr (nblocks + 1) and idx on the device in *ptr_out / *idx_out,
 // allocated from the result's arena by the caller-supplied allocator.
-int one_side(gsofa_ctx* ctx, Scratch& S, int32_t n, long long nblocks, const int64_t* ptr,
+int one_side(gsofa_ctx* ctx, DeviceScratch& S, int32_t n, long long nblocks, const int64_t* ptr,
              const int32_t* idx, const int32_t* blk, const int32_t* start, int64_t* out_ptr,
              int32_t** out_idx, long long* out_count) {
     cudaStream_t st = ctx->stream;
@@ -187,7 +173,7 @@ int build(gsofa_result* r) {
                        "supernodal form needs GSOFA_PATTERN and GSOFA_SUPERNODES");
     const int32_t n = r->n;
     cudaStream_t st = ctx->stream;
-    Scratch S{ctx, {}};
+    DeviceScratch S(ctx);
     int32_t* f01 = static_cast<int32_t*>(S.get(4 * ((size_t)n + 1)));
     int32_t* blk = static_cast<int32_t*>(S.get(4 * ((size_t)n + 1)));
     if (!f01 || !blk) return GSOFA_ERR_OOM_BUDGET;

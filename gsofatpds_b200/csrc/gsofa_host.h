@@ -117,6 +117,11 @@ int parse_dat_files(gsofa_ctx* ctx, const char* beg_file, const char* end_file,
                     const char* csr_file, int32_t* n, int64_t* nnz, std::vector<int32_t>* beg,
                     std::vector<int32_t>* end, std::vector<int32_t>* col);
 int cuda_fail(gsofa_ctx* ctx, cudaError_t e, const char* where);
+// The context's device status word (DEV_ERR_*) and work counter; the
+// status is read back into ctx->h_status and turned into a code by
+// check_status.
+int32_t* work_counter_status(gsofa_ctx* ctx, unsigned long long** wc);
+int check_status(gsofa_ctx* ctx);
 // Pool allocation with budget accounting, ordered on `stream`; the caller
 // holds ctx->mu.
 int dev_alloc_on(gsofa_ctx* ctx, size_t bytes, void** p, cudaStream_t stream);
@@ -137,9 +142,40 @@ MatDesc make_desc(const gsofa_matrix* m, const gsofa_result* r, long long base);
 int ingest_csr(gsofa_ctx* ctx, cudaStream_t stream, int32_t* dstatus, int32_t n, int64_t nnz,
                const int32_t* row_begin, const int32_t* row_end, const int32_t* col,
                gsofa_matrix** out);
+// A matrix handle and its device block for n rows, `real` entries and
+// `padded` padded entries of A (rows rounded up to multiples of 4).
+int matrix_alloc(gsofa_ctx* ctx, cudaStream_t stream, int32_t n, int64_t real, int64_t padded,
+                 int nplanes, gsofa_matrix** out);
+void matrix_free_on(gsofa_matrix* m, cudaStream_t stream);
+// Queues the padded-CSR build of A and A^T on `stream`: m->rowptr (encoded)
+// must already be on the device (or queued); row v of the input is
+// dcol_in[dbeg[v] ...] with the length m->rowptr gives it.
+int matrix_build(gsofa_ctx* ctx, cudaStream_t stream, int32_t* dstatus, gsofa_matrix* m,
+                 int64_t nnz_in, const int32_t* dbeg, const int32_t* dcol_in, int check_symmetry);
 // Device bytes ingest_csr holds for a matrix (kept) and while it runs (staging).
 void ingest_bytes(int32_t n, int64_t nnz, size_t* kept, size_t* staging);
 size_t result_bytes(int32_t n, uint32_t flags);
+
+// Device blocks from the context's pool, released (stream-ordered on the
+// context's stream) when the object goes out of scope.  get() returns null
+// when the budget is exceeded.
+struct DeviceScratch {
+    gsofa_ctx* ctx;
+    std::vector<std::pair<void*, size_t>> blocks;
+    explicit DeviceScratch(gsofa_ctx* c) : ctx(c) {}
+    DeviceScratch(const DeviceScratch&) = delete;
+    DeviceScratch& operator=(const DeviceScratch&) = delete;
+    void* get(size_t bytes) {
+        const size_t b = bytes < 16 ? 16 : bytes;
+        void* p = nullptr;
+        if (dev_alloc_on(ctx, b, &p, ctx->stream)) return nullptr;
+        blocks.emplace_back(p, b);
+        return p;
+    }
+    ~DeviceScratch() {
+        for (auto& b : blocks) dev_free_on(ctx, b.first, b.second, ctx->stream);
+    }
+};
 
 constexpr int kDefaultBuAlpha = 0;  // top-down only unless a caller asks
 constexpr int kDefaultBuBeta = 24;

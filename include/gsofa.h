@@ -130,6 +130,36 @@ int gsofa_load_csr_binary(gsofa_ctx* ctx, const char* path, gsofa_matrix** out);
 int gsofa_matrix_info(const gsofa_matrix* mat, int32_t* n, int64_t* nnz);
 int gsofa_matrix_destroy(gsofa_matrix* mat);
 
+/* ---- fill-reducing ordering (the step before the reference: its inputs are
+ * already permuted by SuperLU_DIST, README.md:27-33; no counterpart in its
+ * code) */
+typedef struct gsofa_order_stats {
+    int32_t rounds;              /* dissection rounds run                      */
+    int32_t splits;              /* components cut by a separator              */
+    int64_t separator_vertices;  /* vertices placed in separators              */
+    int32_t max_separator;       /* largest separator                          */
+    int32_t reserved;
+    double ms;                   /* device time of the ordering                */
+} gsofa_order_stats;
+/* Level-set nested dissection of the structure of A + A^T, on the device:
+ * every round splits each part into its connected components, places the
+ * components of at most leaf_size vertices (ids ascending), and cuts each
+ * larger one at the middle level of a BFS from a pseudo-peripheral vertex
+ * (the separator trimmed to the vertices adjacent to the next level; George
+ * 1973, George and Liu 1981 ch. 8), the two sides first and the separator
+ * last.  Deterministic: the same matrix always gives the same perm.
+ * perm (host, n entries): new index k holds old index perm[k].
+ * leaf_size <= 0 means 32; max_rounds <= 0 means 512 (the last round places
+ * every remaining component whole).  stats may be NULL. */
+int gsofa_order_nd(gsofa_ctx* ctx, const gsofa_matrix* mat, int32_t leaf_size, int32_t max_rounds,
+                   int32_t* perm, gsofa_order_stats* stats);
+/* The symmetrically permuted matrix P A P^T built on the device: row k of
+ * *out is row perm[k] of mat with every column id c renamed to the k' with
+ * perm[k'] = c.  perm: host, n entries, a permutation of 0..n-1 (else
+ * GSOFA_ERR_ARG). */
+int gsofa_matrix_permute(gsofa_ctx* ctx, const gsofa_matrix* mat, const int32_t* perm,
+                         gsofa_matrix** out);
+
 /* ---- factorization (replaces the group loop :2965-3218 and its kernels) --- */
 /* Synchronous: returns when the result is complete on the device. */
 int gsofa_factor_symbolic(gsofa_ctx* ctx, const gsofa_matrix* mat, const gsofa_opts* opts,

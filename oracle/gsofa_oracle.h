@@ -75,6 +75,15 @@ int or_rows(int32_t n, const int32_t* beg, const int32_t* end, const int32_t* co
 int64_t or_supernodes(int32_t n, const int32_t* nzU, const uint32_t* lback,
                       int32_t mss, int8_t* flags);
 
+/* Fill-reducing ordering by level-set nested dissection of A + A^T (the
+ * rule is stated in gsofa_order_oracle.c).  perm (n entries): new index k
+ * holds old index perm[k].  leaf >= 1: components of at most `leaf`
+ * vertices are not split; round max_rounds - 1 places every component.
+ * stats (optional, 4 entries): rounds, splits, separator vertices, largest
+ * separator.  Returns 0, or -1 on bad arguments / allocation failure. */
+int or_order_nd(int32_t n, const int32_t* beg, const int32_t* end, const int32_t* col,
+                int32_t leaf, int32_t max_rounds, int32_t* perm, int64_t* stats);
+
 /* Parse the reference's ASCII files (csr: "E N" then E ids; beg/end: n ids).
  * Allocates *beg,*end,*col with malloc; caller frees with or_free.
  * Returns 0 or -1. */

@@ -40,6 +40,9 @@ def lib():
                                                           ctypes.POINTER(ctypes.c_int64)] + \
             [ctypes.POINTER(ctypes.POINTER(ctypes.c_int32))] * 3
         L.or_free.argtypes = [vp]
+        L.or_order_nd.restype = ctypes.c_int
+        L.or_order_nd.argtypes = [ctypes.c_int32, vp, vp, vp, ctypes.c_int32, ctypes.c_int32, vp,
+                                  vp]
         _lib = L
     return _lib
 
@@ -107,6 +110,23 @@ def supernodes(nzU_ref, lback, mss):
     if c < 0:
         raise ValueError("oracle: bad supernode arguments")
     return int(c), flags
+
+
+def order_nd(beg, end, col, leaf=32, max_rounds=512):
+    """Level-set nested dissection of A + A^T (gsofa_order_oracle.c).
+    Returns (perm, stats): new index k <- old perm[k]; stats = (rounds,
+    splits, separator vertices, largest separator)."""
+    b = np.ascontiguousarray(beg, dtype=np.int32)
+    e = np.ascontiguousarray(end, dtype=np.int32)
+    c = np.ascontiguousarray(col, dtype=np.int32)
+    n = b.shape[0]
+    perm = np.zeros(max(n, 1), np.int32)
+    stats = np.zeros(4, np.int64)
+    rc = lib().or_order_nd(n, _p(b), _p(e), _p(c), int(leaf), int(max_rounds), _p(perm),
+                           _p(stats))
+    if rc != 0:
+        raise ValueError("oracle: bad ordering arguments")
+    return perm[:n], tuple(int(x) for x in stats)
 
 
 def read_dat(beg_file, end_file, csr_file):
