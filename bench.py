@@ -40,6 +40,9 @@ WORKLOADS = {
               "binary CSR file and from host memory (upload, padded CSR of A and A^T, checks)",
     "handoff": "supernodal block form (gsofa_result_supernodal) of the n=20000 random matrix and the "
                "64^3 ND grid, from their materialised patterns, mss 128",
+    "order": "fill-reducing ordering (gsofa_order_nd, level-set nested dissection of A + A^T, leaf 32) "
+             "of the 64^3 7-point grid under a seeded random symmetric permutation (n=262144), "
+             "the n=20000 random matrix and the circuit-like n=659033 matrix",
     "serve": "Poisson request stream, n log-uniform [1000, 1000000], 5-27 nnz/row: 2D 5/9-point and "
              "3D 7/27-point ND grids, random-banded unsymmetric (n capped), 40 GB budget, mss 128",
 }
@@ -331,6 +334,79 @@ def run_handoff(args, local):
     print(json.dumps(line), flush=True)
 
 
+def run_order(args, local):
+    """Ordering on the device against the oracle's single-thread ordering;
+    the fill of each ordered matrix is measured by factoring it on the
+    device (the 64^3 grid also against its coordinate-bisection ND order)."""
+    import torch
+    from gsofatpds_b200 import Context, gen
+    from gsofatpds_b200.gen import csr_to_beg_end
+    from oracle import oracle as O  # the CPU-baseline leg: timed and compared, never shipped
+    torch.cuda.set_device(local)
+    out = {}
+    rng = np.random.default_rng(3)
+    _, rp, col = gen.grid_nd((64, 64, 64), "7")
+    gb, ge = csr_to_beg_end(rp)
+    p = rng.permutation(len(gb)).astype(np.int32)
+    ip = np.empty_like(p)
+    ip[p] = np.arange(len(p), dtype=np.int32)
+    deg = (ge - gb)[p]
+    srp = np.zeros(len(p) + 1, np.int64)
+    np.cumsum(deg, out=srp[1:])
+    scol = np.concatenate([ip[col[gb[v]:ge[v]]] for v in p]).astype(np.int32)
+    cases = [("grid3d_64_scrambled", srp.astype(np.int32), scol, (rp, col)),
+             ("random_extra_20k",) + tuple(gen.random_extra(20000, 3, seed=1)[1:]) + (None,),
+             ("circuit_like",) + tuple(gen.circuit_like()[1:]) + (None,)]
+    with Context(local) as ctx:
+        for name, crp, ccol, nd_ref in cases:
+            m = ctx.load_rowptr(crp, ccol)
+            ms, wall = [], []
+            for it in range(args.warmup + args.steps):
+                t0 = time.perf_counter()
+                perm, st = ctx.order_nd(m)
+                w = (time.perf_counter() - t0) * 1e3
+                if it >= args.warmup:
+                    ms.append(st["ms"])
+                    wall.append(w)
+            row = dict(n=int(m.n), ms_device=float(np.median(ms)), ms_call=float(np.median(wall)),
+                       rounds=st["rounds"], splits=st["splits"],
+                       separator_vertices=st["separator_vertices"],
+                       max_separator=st["max_separator"])
+            b, e = csr_to_beg_end(crp)
+            t0 = time.perf_counter()
+            ref, _ = O.order_nd(b, e, ccol)
+            row["cpu_oracle_ms"] = (time.perf_counter() - t0) * 1e3
+            row["equal_to_oracle"] = bool(np.array_equal(ref, perm))
+            if name != "circuit_like" or args.order_factor_all:
+                pm = ctx.permute(m, perm)
+                r = ctx.factor(pm)
+                row["fill_ordered"] = int(r.counts["fill_count"])
+                row["factor_ms_ordered"] = float(r.counts["ms_device"])
+                r.close()
+                pm.close()
+            if nd_ref is not None:
+                m2 = ctx.load_rowptr(*nd_ref)
+                r = ctx.factor(m2)
+                row["fill_coordinate_nd"] = int(r.counts["fill_count"])
+                r.close()
+                m2.close()
+            elif name != "circuit_like" or args.order_factor_all:
+                r = ctx.factor(m)
+                row["fill_given_order"] = int(r.counts["fill_count"])
+                r.close()
+            m.close()
+            out[name] = row
+    head = out["grid3d_64_scrambled"]
+    line = {"metric": "ordering_ms", "value": head["ms_device"], "unit": "ms", "n_gpus": 1,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": head["ms_device"],
+            "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "int32",
+            "data": "synthetic", "config": {"workload": WORKLOADS["order"]},
+            "cpu_baseline": {"value": head["cpu_oracle_ms"], "unit": "ms", "cores": 1,
+                             "kind": "port", "sample": "the same ordering by the oracle"},
+            "cases": out}
+    print(json.dumps(line), flush=True)
+
+
 def _pct(xs, q):
     return float(np.percentile(np.asarray(xs, dtype=np.float64), q)) if len(xs) else None
 
@@ -445,6 +521,8 @@ def main():
     ap.add_argument("--serve-rate", type=float, default=20.0, help="Poisson arrivals per second")
     ap.add_argument("--serve-max-banded", type=int, default=100000,
                     help="largest random-banded request (their fill grows as n^2)")
+    ap.add_argument("--order-factor-all", action="store_true",
+                    help="order workload: also factor the circuit-like matrix in both orders")
     args = ap.parse_args()
 
     rank = int(os.environ.get("RANK", "0"))
@@ -465,6 +543,9 @@ def main():
         return
     if args.workload == "handoff":
         run_handoff(args, local)
+        return
+    if args.workload == "order":
+        run_order(args, local)
         return
 
     import torch
