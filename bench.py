@@ -43,6 +43,9 @@ WORKLOADS = {
     "order": "fill-reducing ordering (gsofa_order_nd, level-set nested dissection of A + A^T, leaf 32) "
              "of the 64^3 7-point grid under a seeded random symmetric permutation (n=262144), "
              "the n=20000 random matrix and the circuit-like n=659033 matrix",
+    "steal": "the 512-matrix batch mix as 32 chunks of 16 matrices spread over the ranks by "
+             "longest-first per-rank queues with work stealing; each claimed chunk is one batched "
+             "launch (shape from gsofa_autotune_batch)",
     "serve": "Poisson request stream, n log-uniform [1000, 1000000], 5-27 nnz/row: 2D 5/9-point and "
              "3D 7/27-point ND grids, random-banded unsymmetric (n capped), 40 GB budget, mss 128",
 }
@@ -407,6 +410,92 @@ def run_order(args, local):
     print(json.dumps(line), flush=True)
 
 
+def run_steal(args, rank, world, local):
+    """Replicas with per-rank request queues and work stealing: each step
+    spreads the 512-matrix mix (32 chunks of 16) over the ranks; a rank
+    factors its own chunks, then steals from the others' queue heads.  The
+    queue heads live in a TCPStore (host fetch-and-add); the only
+    collectives are the barrier and the max over ranks of the step time."""
+    import torch
+    import torch.distributed as dist
+    from datetime import timedelta
+    from gsofatpds_b200 import Context, gen, replicas
+    torch.cuda.set_device(local)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600),
+                                device_id=torch.device("cuda", local))
+        host = os.environ.get("MASTER_ADDR", "127.0.0.1")
+        port = int(os.environ["MASTER_PORT"]) + 1
+    else:
+        import socket
+        sk = socket.socket()
+        sk.bind(("127.0.0.1", 0))
+        host, port = "127.0.0.1", sk.getsockname()[1]
+        sk.close()
+    store = dist.TCPStore(host, port, world, rank == 0, timeout=timedelta(seconds=600))
+    mats_np = gen.batch_mix(512)
+    chunk = 16
+    chunks = [list(range(i, min(i + chunk, len(mats_np)))) for i in range(0, len(mats_np), chunk)]
+    costs = [sum(int(mats_np[j][2].shape[0]) for j in c) for c in chunks]
+    queues = replicas.assign_queues(costs, world)
+    ctx = Context(local)
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
+    ctx.set_stream(stream.cuda_stream)
+    mats = [ctx.load_rowptr(rp, col) for (_, rp, col) in mats_np]
+    kw = dict(max_supernode_size=128)
+    if not args.no_tune:
+        kw.update(ctx.autotune_batch(mats, **kw))
+    stolen = []
+
+    def step(tag):
+        sq = replicas.StealingQueue(store, rank, world, queues, prefix="bench/steal/%s" % tag)
+        for c in sq:
+            for r in ctx.factor_batch([mats[j] for j in chunks[c]], **kw):
+                r.close()
+        return sq.stolen
+
+    for w in range(args.warmup):
+        if world > 1:
+            dist.barrier()
+        step("w%d" % w)
+    step_ms = []
+    for s_ in range(args.steps):
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        st = step("s%d" % s_)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        step_ms.append(e0.elapsed_time(e1))
+        stolen.append(st)
+    local_ms = float(sum(step_ms))
+    max_ms = replicas.max_over_ranks(local_ms, dist if world > 1 else None, "cuda")
+    stolen_total = int(store.add("bench/steal/stolen", int(sum(stolen))))
+    if world > 1:
+        dist.barrier()
+        stolen_total = int(store.add("bench/steal/stolen", 0))
+    value = replicas.job_throughput(1, args.steps, len(mats), max_ms)
+    if rank == 0:
+        line = {"metric": "matrices_per_s", "value": value, "unit": "matrices/s", "n_gpus": world,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": max_ms / args.steps,
+                "higher_is_better": True, "scaling": "strong", "vs_baseline": None,
+                "dtype": "int32", "data": "synthetic",
+                "config": {"workload": WORKLOADS["steal"], "launch": kw,
+                           "parallelism": "replicas with work stealing"},
+                "chunks_stolen": stolen_total, "chunks_per_step": len(chunks)}
+        print(json.dumps(line), flush=True)
+    for m in mats:
+        m.close()
+    ctx.close()
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
 def _pct(xs, q):
     return float(np.percentile(np.asarray(xs, dtype=np.float64), q)) if len(xs) else None
 
@@ -546,6 +635,9 @@ def main():
         return
     if args.workload == "order":
         run_order(args, local)
+        return
+    if args.workload == "steal":
+        run_steal(args, rank, world, local)
         return
 
     import torch

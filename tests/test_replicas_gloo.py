@@ -57,3 +57,73 @@ def test_single_process_defaults():
     assert replicas.max_over_ranks(12.5) == 12.5
     assert replicas.job_throughput(1, 2, 10.0, 1000.0) == 20.0
     assert replicas.same_input_on_all_ranks(7)
+
+
+def _steal_worker(rank, world, port, q, queues, costs_ms):
+    import time
+    from gsofatpds_b200 import replicas
+    from datetime import timedelta
+    store = dist.TCPStore("127.0.0.1", port, world, rank == 0, timeout=timedelta(seconds=60))
+    sq = replicas.StealingQueue(store, rank, world, queues)
+    store.add("gsofa/steal/ready", 1)  # start together
+    while int(store.add("gsofa/steal/ready", 0)) < world:
+        time.sleep(0.005)
+    done = []
+    t0 = time.perf_counter()
+    for req in sq:
+        time.sleep(costs_ms[req] / 1e3)
+        sq.publish(req, {"req": req, "rank": rank})
+        done.append(req)
+    busy = time.perf_counter() - t0
+    owners = sq.owners(len(costs_ms))
+    res = sq.results(len(costs_ms))
+    store.add("gsofa/steal/exit", 1)
+    if rank == 0:  # the store's server lives in rank 0: wait for every reader
+        store.wait(["gsofa/steal/exit"])
+        while int(store.add("gsofa/steal/exit", 0)) < world:
+            time.sleep(0.01)
+    q.put((rank, done, sq.stolen, busy, owners, [r["rank"] for r in res]))
+
+
+def _run_steal(world, queues, costs_ms):
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_steal_worker, args=(r, world, port, q, queues, costs_ms))
+             for r in range(world)]
+    for p in procs:
+        p.start()
+    res = sorted([q.get(timeout=120) for _ in range(world)])
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    return res
+
+
+def test_work_stealing_every_request_exactly_once():
+    """Every request lands in rank 0's queue; the idle ranks steal from its
+    head (victims rank+1+k), and each request is processed exactly once."""
+    world = 3
+    costs = [30.0] * 12
+    res = _run_steal(world, [list(range(12)), [], []], costs)
+    done = [set(r[1]) for r in res]
+    assert set().union(*done) == set(range(12))
+    assert sum(len(d) for d in done) == 12
+    assert res[1][2] > 0 and res[2][2] > 0  # ranks 1 and 2 stole
+    assert res[0][2] == 0
+    for rank, d, _, _, owners, published in res:
+        for req in d:
+            assert owners[req] == rank and published[req] == rank
+    # balanced by stealing: no rank did much more than its share
+    assert max(len(d) for d in done) <= 6
+
+
+def test_longest_first_queues():
+    from gsofatpds_b200 import replicas
+    costs = [5, 1, 9, 3, 3, 7, 2]
+    qs = replicas.assign_queues(costs, 3)
+    assert sorted(i for q in qs for i in q) == list(range(7))
+    loads = [sum(costs[i] for i in q) for q in qs]
+    assert max(loads) - min(loads) <= max(costs)
+    assert qs[0][0] == 2 and qs[1][0] == 5  # largest first, lowest rank on ties
+    assert replicas.assign_queues([], 2) == [[], []]
