@@ -933,6 +933,11 @@ static int autotune_impl(gsofa_ctx* ctx, const gsofa_matrix* const* mats, int32_
         }
         int e = run_factor(ctx, mats, count, &p, rr.data(), stride);
         *ms = e ? 1e300 : rr[0]->counts.ms_traverse;
+        if (e) {
+            const std::string prev = ctx->err;
+            set_err(ctx, e, "%s; timing threads %d, ring %d, chunk %d, heavy row %d", prev.c_str(),
+                    c.block, p.cached_closures, p.chunk_sources, p.heavy_row);
+        }
         return e;
     };
     // coordinate descent from the defaults: CTA size, closure ring, chunk,

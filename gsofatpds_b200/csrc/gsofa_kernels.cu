@@ -708,7 +708,13 @@ __global__ void __launch_bounds__(BLOCK, 1024 / BLOCK) traverse_kernel(TraverseL
                     SM.item = got ? it : -1;
                 }
             }
-        } else if (threadIdx.x == 0) {
+        } else {
+            // every thread is done with the previous item's descriptor before
+            // thread 0 replaces it (an empty item, e.g. the direction-1 half
+            // of a symmetric matrix, has no source-loop barrier of its own)
+            __syncthreads();
+        }
+        if (MODE != 2 && threadIdx.x == 0) {
             const unsigned long long c = atomicAdd(P.work_counter, 1ull);
             const long long it = (long long)c < P.total_items ? (long long)c : -1;
             if (it >= 0) {

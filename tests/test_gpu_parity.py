@@ -326,6 +326,32 @@ def test_autotune_batch_shapes_give_the_same_results(ctx):
         m.close()
 
 
+def test_batch_of_symmetric_matrices_repeated(ctx):
+    """Every direction-1 item of a symmetric matrix is empty (the direction-0
+    item fills both halves), so a batch of grids hands each CTA many items
+    with no source loop in a row.  Each CTA must finish reading an item's
+    descriptor before it takes the next one: repeated launches must all
+    succeed with the alone results."""
+    from gsofatpds_b200 import gen
+    mats_np = [gen.grid_nd((s, s + 3), "5" if s % 2 else "9") for s in range(20, 60, 4)]
+    mats_np += [gen.random_banded(3000, bw=6, extra=2, seed=5)]
+    mats = [ctx.load_rowptr(rp, col) for (_, rp, col) in mats_np]
+    ref = []
+    for m in mats:
+        r = ctx.factor(m)
+        ref.append((r.counts["fill_count"], r.row_counts()["nnz_u_row"]))
+        r.close()
+    for rep in range(25):
+        tps = (256, 512, 1024)[rep % 3]
+        rs = ctx.factor_batch(mats, chunk_sources=16, threads_per_source=tps)
+        for (fill, urow), r in zip(ref, rs):
+            assert r.counts["fill_count"] == fill, rep
+            np.testing.assert_array_equal(r.row_counts()["nnz_u_row"], urow)
+            r.close()
+    for m in mats:
+        m.close()
+
+
 def test_batch_equals_alone(ctx):
     from gsofatpds_b200 import gen
     mats_np = [gen.grid_nd((40, 37), "5"), gen.random_banded(2500, bw=5, extra=1, seed=2),
