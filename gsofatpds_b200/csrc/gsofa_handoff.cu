@@ -9,12 +9,13 @@
 //   U cols  = { c >= l : U(r, c) != 0 for some row r of the block }
 // both sorted; the diagonal block itself is dense and implicit.  They are
 // built from the materialised pattern (L by columns, U by rows) with no
-// per-block bitmaps: every (block, index) pair is emitted as one 64-bit key,
-// radix-sorted and made unique, and each block's range is found by binary
-// search on the block id.
-#include <cub/device/device_radix_sort.cuh>
+// per-block bitmaps.  The ids at or past each list's block end are emitted
+// list after list, so every block's ids form one contiguous segment; a
+// segmented sort of the 32-bit ids, a head flag per new value (the first of
+// a segment, or one that differs from its predecessor) and a scan of the
+// flags give each block's sorted union and its offset.
 #include <cub/device/device_scan.cuh>
-#include <cub/device/device_select.cuh>
+#include <cub/device/device_segmented_sort.cuh>
 
 #include <algorithm>
 
@@ -70,7 +71,7 @@ __global__ void count_kernel(int32_t n, const int64_t* __restrict__ ptr,
 __global__ void emit_kernel(int32_t n, const int64_t* __restrict__ ptr,
                             const int32_t* __restrict__ idx, const int32_t* __restrict__ blk,
                             const int32_t* __restrict__ start, const long long* __restrict__ off,
-                            unsigned long long* __restrict__ keys) {
+                            int32_t* __restrict__ ids) {
     const int lane = threadIdx.x & 31;
     const long long gw = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
@@ -78,33 +79,48 @@ __global__ void emit_kernel(int32_t n, const int64_t* __restrict__ ptr,
         const int32_t l = start[blk[c] + 1];
         const long long b = ptr[c], e = ptr[c + 1];
         const long long first = lower_bound_i32(idx, b, e, l);
-        const unsigned long long hi = (unsigned long long)(uint32_t)blk[c] << 32;
-        for (long long j = first + lane; j < e; j += 32)
-            keys[off[c] + (j - first)] = hi | (uint32_t)idx[j];
+        for (long long j = first + lane; j < e; j += 32) ids[off[c] + (j - first)] = idx[j];
     }
 }
 
-// out_ptr[k] = first unique key of block k (binary search); out_idx = low words
-__global__ void block_ptr_kernel(long long nblocks, const unsigned long long* __restrict__ ukeys,
-                                 long long nu, int64_t* __restrict__ out_ptr) {
+// seg[k] = where block k's ids start (its first list's offset); seg[nb] = total
+__global__ void segment_kernel(long long nblocks, const int32_t* __restrict__ start,
+                               const long long* __restrict__ off, int32_t* __restrict__ seg) {
     for (long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x; k <= nblocks;
-         k += (long long)gridDim.x * blockDim.x) {
-        const unsigned long long x = (unsigned long long)k << 32;
-        long long lo = 0, hi = nu;
-        while (lo < hi) {
-            const long long mid = (lo + hi) >> 1;
-            if (ukeys[mid] < x) lo = mid + 1;
-            else hi = mid;
-        }
-        out_ptr[k] = lo;
-    }
+         k += (long long)gridDim.x * blockDim.x)
+        seg[k] = (int32_t)off[start[k]];
 }
 
-__global__ void low_word_kernel(long long count, const unsigned long long* __restrict__ ukeys,
-                                int32_t* __restrict__ out) {
+// flag[i] = 1 when sorted[i] opens a segment or differs from sorted[i-1]
+// (head[i] marks segment starts)
+__global__ void new_value_kernel(long long count, const int32_t* __restrict__ sorted,
+                                 const int8_t* __restrict__ head, int32_t* __restrict__ flag) {
     for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < count;
          i += (long long)gridDim.x * blockDim.x)
-        out[i] = (int32_t)(uint32_t)ukeys[i];
+        flag[i] = (i == 0 || head[i] || sorted[i] != sorted[i - 1]) ? 1 : 0;
+}
+
+__global__ void head_kernel(long long nblocks, const int32_t* __restrict__ seg,
+                            int8_t* __restrict__ head) {
+    for (long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x; k < nblocks;
+         k += (long long)gridDim.x * blockDim.x)
+        if (seg[k] < seg[k + 1]) head[seg[k]] = 1;
+}
+
+// out[pos[i]] = sorted[i] for flagged i; out_ptr[k] = pos at block k's start
+__global__ void compact_kernel(long long count, const int32_t* __restrict__ sorted,
+                               const int32_t* __restrict__ flag, const int32_t* __restrict__ pos,
+                               int32_t* __restrict__ out) {
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < count;
+         i += (long long)gridDim.x * blockDim.x)
+        if (flag[i]) out[pos[i]] = sorted[i];
+}
+
+__global__ void block_ptr_kernel(long long nblocks, const int32_t* __restrict__ seg,
+                                 const int32_t* __restrict__ pos, int64_t* __restrict__ out_ptr) {
+    for (long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x; k <= nblocks;
+         k += (long long)gridDim.x * blockDim.x)
+        out_ptr[k] = pos[seg[k]];
 }
 
 int grid_for(long long items, int threads) {
@@ -112,9 +128,8 @@ int grid_for(long long items, int threads) {
     return (int)std::max(1ll, std::min(g, 148ll * 32));
 }
 
-// Unique sorted (block, index) pairs of one side; returns their count and
-// leaves ptr (nblocks + 1) and idx on the device in *ptr_out / *idx_out,
-// allocated from the result's arena by the caller-supplied allocator.
+// Sorted union per block of one side's lists past the block end: fills
+// out_ptr (nblocks + 1) and allocates *out_idx (*out_count ids).
 int one_side(gsofa_ctx* ctx, DeviceScratch& S, int32_t n, long long nblocks, const int64_t* ptr,
              const int32_t* idx, const int32_t* blk, const int32_t* start, int64_t* out_ptr,
              int32_t** out_idx, long long* out_count) {
@@ -133,32 +148,40 @@ int one_side(gsofa_ctx* ctx, DeviceScratch& S, int32_t n, long long nblocks, con
     if (cudaMemcpyAsync(&total, off + n, 8, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
         cudaStreamSynchronize(st) != cudaSuccess)
         return set_err(ctx, GSOFA_ERR_CUDA, "supernodal form: count read-back");
-    if (total > INT32_MAX)
-        return set_err(ctx, GSOFA_ERR_UNSUPPORTED, "supernodal form: more than 2^31 entries");
+    if (total >= INT32_MAX)
+        return set_err(ctx, GSOFA_ERR_UNSUPPORTED, "supernodal form: 2^31 entries or more");
     const int items = (int)total;
-    unsigned long long* keys = static_cast<unsigned long long*>(S.get(8 * (size_t)items));
-    unsigned long long* sorted = static_cast<unsigned long long*>(S.get(8 * (size_t)items));
-    unsigned long long* uniq = static_cast<unsigned long long*>(S.get(8 * (size_t)items));
-    int* nsel = static_cast<int*>(S.get(16));
-    if (!keys || !sorted || !uniq || !nsel) return GSOFA_ERR_OOM_BUDGET;
-    emit_kernel<<<grid_for(32ll * n, 256), 256, 0, st>>>(n, ptr, idx, blk, start, off, keys);
-    int end_bit = 32;
-    while (end_bit < 64 && (1ll << (end_bit - 32)) <= nblocks) end_bit++;
-    size_t sb = 0, ub = 0;
-    cub::DeviceRadixSort::SortKeys(nullptr, sb, keys, sorted, items, 0, end_bit, st);
-    cub::DeviceSelect::Unique(nullptr, ub, sorted, uniq, nsel, items, st);
-    void* tmp2 = S.get(std::max(sb, ub));
+    const size_t I = (size_t)std::max(items, 1);
+    int32_t* ids = static_cast<int32_t*>(S.get(4 * I));
+    int32_t* sorted = static_cast<int32_t*>(S.get(4 * I));
+    int32_t* flag = static_cast<int32_t*>(S.get(4 * (I + 1)));
+    int32_t* pos = static_cast<int32_t*>(S.get(4 * (I + 1)));
+    int8_t* head = static_cast<int8_t*>(S.get(I));
+    int32_t* seg = static_cast<int32_t*>(S.get(4 * ((size_t)nblocks + 1)));
+    if (!ids || !sorted || !flag || !pos || !head || !seg) return GSOFA_ERR_OOM_BUDGET;
+    emit_kernel<<<grid_for(32ll * n, 256), 256, 0, st>>>(n, ptr, idx, blk, start, off, ids);
+    segment_kernel<<<grid_for(nblocks + 1, 256), 256, 0, st>>>(nblocks, start, off, seg);
+    size_t sb = 0, pb = 0;
+    cub::DeviceSegmentedSort::SortKeys(nullptr, sb, ids, sorted, items, (int)nblocks, seg, seg + 1,
+                                       st);
+    cub::DeviceScan::ExclusiveSum(nullptr, pb, flag, pos, items + 1, st);
+    void* tmp2 = S.get(std::max(sb, pb));
     if (!tmp2) return GSOFA_ERR_OOM_BUDGET;
-    cub::DeviceRadixSort::SortKeys(tmp2, sb, keys, sorted, items, 0, end_bit, st);
-    cub::DeviceSelect::Unique(tmp2, ub, sorted, uniq, nsel, items, st);
+    cub::DeviceSegmentedSort::SortKeys(tmp2, sb, ids, sorted, items, (int)nblocks, seg, seg + 1,
+                                       st);
+    cudaMemsetAsync(head, 0, I, st);
+    head_kernel<<<grid_for(nblocks, 256), 256, 0, st>>>(nblocks, seg, head);
+    cudaMemsetAsync(flag + items, 0, 4, st);
+    new_value_kernel<<<grid_for(items, 256), 256, 0, st>>>(items, sorted, head, flag);
+    cub::DeviceScan::ExclusiveSum(tmp2, pb, flag, pos, items + 1, st);
     int nu = 0;
-    if (cudaMemcpyAsync(&nu, nsel, 4, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+    if (cudaMemcpyAsync(&nu, pos + items, 4, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
         cudaStreamSynchronize(st) != cudaSuccess)
         return set_err(ctx, GSOFA_ERR_CUDA, "supernodal form: unique count read-back");
-    block_ptr_kernel<<<grid_for(nblocks + 1, 256), 256, 0, st>>>(nblocks, uniq, nu, out_ptr);
+    block_ptr_kernel<<<grid_for(nblocks + 1, 256), 256, 0, st>>>(nblocks, seg, pos, out_ptr);
     int32_t* dst = nullptr;
     if (dev_alloc_on(ctx, 4 * (size_t)std::max(nu, 1), (void**)&dst, st)) return GSOFA_ERR_OOM_BUDGET;
-    low_word_kernel<<<grid_for(nu, 256), 256, 0, st>>>(nu, uniq, dst);
+    compact_kernel<<<grid_for(items, 256), 256, 0, st>>>(items, sorted, flag, pos, dst);
     *out_idx = dst;
     *out_count = nu;
     return cudaGetLastError() == cudaSuccess ? GSOFA_OK
