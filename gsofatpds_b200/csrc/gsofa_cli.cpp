@@ -7,13 +7,17 @@
 // Two more modes for the binary CSR files of include/gsofa.h:
 //   gsofa_cli --convert beg end csr out.gsofacsr   (parse once, no GPU)
 //   gsofa_cli --binary file.gsofacsr max_supernode_size
+// and one that orders the matrix on the device first (gsofa_order_nd, then
+// gsofa_matrix_permute) and factors the permuted matrix:
+//   gsofa_cli --order file.gsofacsr max_supernode_size
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <vector>
 
 #include "../../include/gsofa.h"
 
-static int run_binary(const char* path, int mss) {
+static int run_binary(const char* path, int mss, bool order) {
     gsofa_ctx* ctx = nullptr;
     int rc = gsofa_create(0, 0, &ctx);
     if (rc) {
@@ -26,6 +30,23 @@ static int run_binary(const char* path, int mss) {
     gsofa_opts_default(&o);
     o.max_supernode_size = mss;
     rc = gsofa_load_csr_binary(ctx, path, &m);
+    if (rc == GSOFA_OK && order) {
+        int32_t n = 0;
+        int64_t nnz = 0;
+        gsofa_matrix_info(m, &n, &nnz);
+        std::vector<int32_t> perm((size_t)n);
+        gsofa_order_stats st;
+        gsofa_matrix* pm = nullptr;
+        rc = gsofa_order_nd(ctx, m, 0, 0, perm.data(), &st);
+        if (rc == GSOFA_OK) rc = gsofa_matrix_permute(ctx, m, perm.data(), &pm);
+        if (rc == GSOFA_OK) {
+            printf("Ordering (nested dissection on the device): %g ms, %d rounds, %lld separator "
+                   "vertices\n",
+                   st.ms, st.rounds, (long long)st.separator_vertices);
+            gsofa_matrix_destroy(m);
+            m = pm;
+        }
+    }
     if (rc == GSOFA_OK) rc = gsofa_factor_symbolic(ctx, m, &o, &r);
     if (rc != GSOFA_OK) {
         fprintf(stderr, "gsofa_cli: %s (%s)\n", gsofa_status_string(rc), gsofa_last_error(ctx));
@@ -54,15 +75,18 @@ int main(int argc, char** argv) {
         }
         return 0;
     }
-    if (argc == 4 && strcmp(argv[1], "--binary") == 0) return run_binary(argv[2], atoi(argv[3]));
+    if (argc == 4 && strcmp(argv[1], "--binary") == 0)
+        return run_binary(argv[2], atoi(argv[3]), false);
+    if (argc == 4 && strcmp(argv[1], "--order") == 0) return run_binary(argv[2], atoi(argv[3]), true);
     if (argc != 11 && argc != 6) {
         fprintf(stderr,
                 "usage: %s beg end csr #Processes max_supernode_size percent_cat0 percent_cat2 "
                 "N_blocks_source_cat2 N_GPU_Node N_src_group\n"
                 "   or: %s beg end csr N_virtualGPU total_memory_GB\n"
                 "   or: %s --convert beg end csr out.gsofacsr\n"
-                "   or: %s --binary file.gsofacsr max_supernode_size\n",
-                argv[0], argv[0], argv[0], argv[0]);
+                "   or: %s --binary file.gsofacsr max_supernode_size\n"
+                "   or: %s --order file.gsofacsr max_supernode_size\n",
+                argv[0], argv[0], argv[0], argv[0], argv[0]);
         return 1;
     }
     printf("Number of Processes: %s\n", argv[4]);

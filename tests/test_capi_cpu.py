@@ -67,6 +67,18 @@ def test_server_calls_reject_null_handles():
     assert L.gsofa_server_last_error(None) == b"null server"
 
 
+def test_order_and_permute_reject_null_handles():
+    from gsofatpds_b200 import _lib
+    L = _lib.load()
+    st = _lib.OrderStats()
+    h = ctypes.c_void_p()
+    assert L.gsofa_order_nd(None, None, 0, 0, None, ctypes.byref(st)) == _lib.ERR_ARG
+    assert L.gsofa_matrix_permute(None, None, None, ctypes.byref(h)) == _lib.ERR_ARG
+    nb = ctypes.c_int64()
+    assert L.gsofa_result_supernodal(None, ctypes.byref(nb), None, None, None, None, None, None,
+                                     None) == _lib.ERR_ARG
+
+
 def test_cli_usage_without_arguments():
     from gsofatpds_b200 import _lib
     out = subprocess.run([_lib.CLI_PATH], capture_output=True, text=True, timeout=60)

@@ -310,3 +310,22 @@ def test_permute_then_factor(ctx):
     with pytest.raises(GsofaError):
         ctx.permute(m, bad)
     m.close()
+
+
+@pytest.mark.gpu
+def test_cli_order_mode(tmp_path):
+    """gsofa_cli --order: binary file -> device ordering -> P A P^T -> factor;
+    the fill equals the oracle's on the same permutation."""
+    import subprocess
+    _cuda()
+    from gsofatpds_b200 import _lib, write_binary
+    b, e, c = _grid2d(50, 40, np.random.default_rng(9))
+    path = str(tmp_path / "g.gsofacsr")
+    write_binary(path, b, e, c)
+    out = subprocess.run([_lib.CLI_PATH, "--order", path, "128"], capture_output=True, text=True,
+                         timeout=300)
+    assert out.returncode == 0, out.stderr
+    perm, _ = O.order_nd(b, e, c, leaf=32)
+    ref = _fill(*permuted(b, e, c, perm))
+    assert "Final Number of fill-ins detected: %d" % ref in out.stdout, out.stdout
+    assert "Ordering (nested dissection on the device)" in out.stdout
