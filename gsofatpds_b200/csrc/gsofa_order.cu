@@ -32,11 +32,13 @@
 //               its smallest id, whatever order the hooks ran in;
 //   ranges      roots keyed (part, root), radix-sorted, sizes exclusive-
 //               scanned, each part's first key found by binary search;
-//   BFS         one cooperative launch per search, all parts' searches
-//               level-synchronous together: warp per frontier vertex,
-//               compare-and-swap on the distance, block-local queue flushed
-//               with one atomic per block per level, a grid barrier whose
-//               wait is bounded (GSOFA_ERR_TIMEOUT past 2 s);
+//   BFS         parts above 2048 vertices: one cooperative launch per
+//               search, all their searches level-synchronous together: warp
+//               per frontier vertex, compare-and-swap on the distance,
+//               block-local queue flushed with one atomic per block per
+//               level, a grid barrier whose wait is bounded (GSOFA_ERR_TIMEOUT
+//               past 2 s); smaller parts: the whole search inside one CTA
+//               (block barriers only), queued in the part's own slice;
 //   levels      per part, level sizes are counted into the part's own slice
 //               of a histogram (lo + level < lo + |part|), one warp per part
 //               scans it for m and e;
@@ -62,6 +64,8 @@ constexpr int kBfsThreads = 512;
 constexpr int kBfsBlocksPerSm = 2;
 constexpr int kBlockQueue = 2048;                         // block-local BFS queue entries
 constexpr unsigned long long kBarrierLimitNs = 2000000000ull;  // one grid barrier wait
+constexpr int kLocalThreads = 512;
+constexpr int32_t kLocalMax = 2048;  // parts up to this size search inside one CTA
 constexpr int32_t kDefaultLeaf = 32;
 constexpr int32_t kDefaultMaxRounds = 512;
 
@@ -228,13 +232,15 @@ __global__ void relabel_kernel(int32_t n, int32_t* __restrict__ part,
 
 // A source outside [0, n) can only follow a search that gave up (the round
 // is then abandoned): it is recorded, not used.
+// Seeds the grid-wide search with the parts above max(leaf, local_max).
 __global__ void bfs_seed_kernel(int R, int32_t n, const int32_t* __restrict__ psize, int32_t leaf,
-                                const int32_t* __restrict__ src, const int32_t* __restrict__ plo,
-                                int32_t* __restrict__ dist, int32_t* __restrict__ q0,
-                                int32_t* lcnt, int32_t* __restrict__ H, int32_t* err) {
+                                int32_t local_max, const int32_t* __restrict__ src,
+                                const int32_t* __restrict__ plo, int32_t* __restrict__ dist,
+                                int32_t* __restrict__ q0, int32_t* lcnt, int32_t* __restrict__ H,
+                                int32_t* err) {
     for (long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x; k < R;
          k += (long long)gridDim.x * blockDim.x) {
-        if (psize[k] <= leaf) continue;
+        if (psize[k] <= leaf || psize[k] <= local_max) continue;
         const int s = src[k];
         if (s < 0 || s >= n) {
             atomicOr(err, 2);
@@ -336,6 +342,67 @@ __global__ void __launch_bounds__(kBfsThreads) bfs_kernel(BfsArgs a) {
         __syncthreads();
         if (threadIdx.x == 0) sq_n = 0;
         if (!grid_barrier(a.bar, a.err)) return;
+    }
+}
+
+// The search of each part of (leaf, local_max] vertices inside one CTA: no
+// grid barrier, one block barrier per level.  The queue is the part's own
+// slice q[plo .. plo + size) (parts are disjoint), level sizes go to
+// H[plo + level] as in the grid-wide search.
+__global__ void __launch_bounds__(kLocalThreads) bfs_local_kernel(
+    Graph g, int R, int32_t n, const int32_t* __restrict__ psize, int32_t leaf, int32_t local_max,
+    const int32_t* __restrict__ src, const int32_t* __restrict__ plo,
+    const int32_t* __restrict__ part, int32_t* dist, int32_t* q, int32_t* __restrict__ H,
+    int32_t* err) {
+    __shared__ int found;
+    const int lane = threadIdx.x & 31;
+    const int warp = threadIdx.x >> 5;
+    constexpr int NW = kLocalThreads / 32;
+    for (int k = blockIdx.x; k < R; k += gridDim.x) {
+        const int size = psize[k];
+        if (size <= leaf || size > local_max) continue;
+        const int base = plo[k];
+        const int s0 = src[k];
+        if (s0 < 0 || s0 >= n) {  // only after a search that gave up
+            if (threadIdx.x == 0) atomicOr(err, 2);
+            continue;
+        }
+        if (threadIdx.x == 0) {
+            dist[s0] = 0;
+            q[base] = s0;
+            H[base] = 1;
+            found = 0;
+        }
+        __syncthreads();
+        int lb = 0, le = 1;
+        for (int L = 0; lb < le; L++) {
+            for (int i = lb + warp; i < le; i += NW) {
+                const int u = q[base + i];
+                for (int side = 0; side < 2; side++) {
+                    const int32_t* rp = side ? g.trp : g.rp;
+                    const int32_t* cl = side ? g.tcol : g.col;
+                    const int b = __ldg(rp + u) & ~3, e = __ldg(rp + u + 1) & ~3;
+                    for (int j = b + lane; j < e; j += 32) {
+                        const int w = __ldg(cl + j);
+                        if (w == u || __ldg(part + w) != k || dist[w] >= 0) continue;
+                        if (atomicCAS(dist + w, -1, L + 1) != -1) continue;
+                        const int pos = le + atomicAdd(&found, 1);
+                        if (pos < size) q[base + pos] = w;
+                        else atomicOr(err, 4);  // a part holds at most `size` vertices
+                    }
+                }
+            }
+            __syncthreads();
+            const int nxt = found;
+            __syncthreads();
+            if (threadIdx.x == 0) {
+                found = 0;
+                if (nxt > 0 && le < size) H[base + L + 1] = nxt;
+            }
+            lb = le;
+            le = min(le + nxt, size);
+            __syncthreads();
+        }
     }
 }
 
@@ -616,13 +683,17 @@ int order_impl(gsofa_ctx* ctx, const gsofa_matrix* mat, int32_t leaf, int32_t ma
         cudaMemsetAsync(lcnt, 0, 4 * (N + 2), st);
         cudaMemsetAsync(H, 0, 4 * N, st);
         cudaMemsetAsync(bar, 0, 8, st);
-        bfs_seed_kernel<<<grid_for(R, kThreads), kThreads, 0, st>>>(R, n, psize, leaf_eff, src,
-                                                                    plo, dist, q0, lcnt, H, err);
+        bfs_seed_kernel<<<grid_for(R, kThreads), kThreads, 0, st>>>(
+            R, n, psize, leaf_eff, kLocalMax, src, plo, dist, q0, lcnt, H, err);
         BfsArgs a{g, part, plo, dist, q0, q1, lcnt, H, bar, err, n + 1};
         void* args[] = {&a};
         cudaError_t e = cudaLaunchCooperativeKernel((const void*)bfs_kernel, dim3(bfs_grid),
                                                     dim3(kBfsThreads), args, 0, st);
-        return e == cudaSuccess ? GSOFA_OK : cuda_fail(ctx, e, "ordering BFS launch");
+        if (e != cudaSuccess) return cuda_fail(ctx, e, "ordering BFS launch");
+        // the smaller parts, one CTA each; q0 is free once the grid-wide search ended
+        bfs_local_kernel<<<std::max(1, std::min(R, ctx->sm_count * 4)), kLocalThreads, 0, st>>>(
+            g, R, n, psize, leaf_eff, kLocalMax, src, plo, part, dist, q0, H, err);
+        return GSOFA_OK;
     };
     cudaMemsetAsync(err, 0, 4, st);
     for (int r = 0; active > 0; r++) {
