@@ -230,10 +230,16 @@ def run_batch(args, local):
         for m, k in zip(mats, plain_kw):
             ctx.factor(m, **k).close()
 
+    def plain_defaults():  # what a caller gets without the tuner
+        for m in mats:
+            ctx.factor(m, **base).close()
+
     for _ in range(args.warmup):
         plain()
+        plain_defaults()
         batch.run()
     plain_ms = [timed(plain) for _ in range(args.steps)]
+    plain_def_ms = [timed(plain_defaults) for _ in range(args.steps)]
     batch_ms = [timed(batch.run) for _ in range(args.steps)]
     edges = sum(batch.result(i).counts["edges_alg"] for i in range(len(mats)))
     pm, bm = float(np.median(plain_ms)), float(np.median(batch_ms))
@@ -244,7 +250,10 @@ def run_batch(args, local):
                                             "launch": {k: v for k, v in kw.items()}},
             "plain_ms_per_batch": pm, "plain_matrices_per_s": len(mats) / (pm / 1e3),
             "plain_shapes": "per-matrix autotuned" if not args.no_tune else "library defaults",
-            "speedup_vs_plain": pm / bm, "edges_alg": edges, "gteps": edges / (bm / 1e3) / 1e9,
+            "speedup_vs_plain": pm / bm,
+            "plain_defaults_ms_per_batch": float(np.median(plain_def_ms)),
+            "speedup_vs_plain_defaults": float(np.median(plain_def_ms)) / bm,
+            "edges_alg": edges, "gteps": edges / (bm / 1e3) / 1e9,
             "gpu_launches": 1}
     print(json.dumps(line), flush=True)
     batch.close()
