@@ -697,6 +697,10 @@ int order_impl(gsofa_ctx* ctx, const gsofa_matrix* mat, int32_t leaf, int32_t ma
     };
     cudaMemsetAsync(err, 0, 4, st);
     for (int r = 0; active > 0; r++) {
+        // the last permitted round places every component, so active reaches
+        // 0 by then; anything else is a failure reported here, not a loop
+        if (r >= max_rounds)
+            return set_err(ctx, GSOFA_ERR_CUDA, "ordering: vertices left after round %d", r);
         rounds++;
         const int32_t leaf_eff = r == max_rounds - 1 ? INT32_MAX : leaf;
         // 1. components of every part
@@ -738,7 +742,8 @@ int order_impl(gsofa_ctx* ctx, const gsofa_matrix* mat, int32_t leaf, int32_t ma
                                                                       pnm, pcnts, plo_next, tot);
         unsigned long long ht[4] = {0, 0, 0, 0};
         int32_t herr = 0;
-        cudaError_t e = cudaMemcpyAsync(ht, tot, 32, cudaMemcpyDeviceToHost, st);
+        cudaError_t e = cudaGetLastError();  // launch errors of this round
+        if (e == cudaSuccess) e = cudaMemcpyAsync(ht, tot, 32, cudaMemcpyDeviceToHost, st);
         if (e == cudaSuccess) e = cudaMemcpyAsync(&herr, err, 4, cudaMemcpyDeviceToHost, st);
         if (e == cudaSuccess) e = cudaStreamSynchronize(st);
         if (e != cudaSuccess) return cuda_fail(ctx, e, "ordering round");
