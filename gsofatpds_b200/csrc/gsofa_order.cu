@@ -264,12 +264,16 @@ struct BfsArgs {
     unsigned* bar;  // [0] arrivals, [1] generation
     int32_t* err;
     int32_t max_levels;
+    unsigned arrivals;             // blocks the barrier waits for (gridDim.x; more only
+                                   // in gsofa_order_wait_selftest, so that the wait runs out)
+    unsigned long long limit_ns;   // one barrier wait gives up after this
 };
 
-// Grid-wide barrier of a cooperative launch (every block is resident).  The
-// wait gives up after kBarrierLimitNs or once another block has given up;
-// then it sets *err and returns false, and the caller returns.
-__device__ bool grid_barrier(unsigned* bar, int32_t* err) {
+// Grid-wide barrier of a cooperative launch (every block is resident) over
+// `arrivals` blocks.  The wait gives up after limit_ns or once another block
+// has given up; then it sets *err and returns false, and the caller returns.
+__device__ bool grid_barrier(unsigned* bar, int32_t* err, unsigned arrivals,
+                             unsigned long long limit_ns) {
     __shared__ int ok;
     __syncthreads();
     if (threadIdx.x == 0) {
@@ -277,15 +281,14 @@ __device__ bool grid_barrier(unsigned* bar, int32_t* err) {
         volatile unsigned* gen = bar + 1;
         const unsigned g0 = *gen;
         __threadfence();
-        if (atomicAdd(bar, 1u) == gridDim.x - 1) {
+        if (atomicAdd(bar, 1u) == arrivals - 1) {
             atomicExch(bar, 0u);
             __threadfence();
             atomicAdd(bar + 1, 1u);
         } else {
             const unsigned long long t0 = global_ns();
             while (*gen == g0) {
-                if (*reinterpret_cast<volatile int32_t*>(err) ||
-                    global_ns() - t0 > kBarrierLimitNs) {
+                if (*reinterpret_cast<volatile int32_t*>(err) || global_ns() - t0 > limit_ns) {
                     atomicOr(err, 1);
                     ok = 0;
                     break;
@@ -341,7 +344,7 @@ __global__ void __launch_bounds__(kBfsThreads) bfs_kernel(BfsArgs a) {
         for (int t = threadIdx.x; t < ns; t += blockDim.x) qout[sq_base + t] = sq[t];
         __syncthreads();
         if (threadIdx.x == 0) sq_n = 0;
-        if (!grid_barrier(a.bar, a.err)) return;
+        if (!grid_barrier(a.bar, a.err, a.arrivals, a.limit_ns)) return;
     }
 }
 
@@ -685,7 +688,8 @@ int order_impl(gsofa_ctx* ctx, const gsofa_matrix* mat, int32_t leaf, int32_t ma
         cudaMemsetAsync(bar, 0, 8, st);
         bfs_seed_kernel<<<grid_for(R, kThreads), kThreads, 0, st>>>(
             R, n, psize, leaf_eff, kLocalMax, src, plo, dist, q0, lcnt, H, err);
-        BfsArgs a{g, part, plo, dist, q0, q1, lcnt, H, bar, err, n + 1};
+        BfsArgs a{g, part, plo, dist, q0, q1, lcnt, H, bar, err, n + 1, (unsigned)bfs_grid,
+                  kBarrierLimitNs};
         void* args[] = {&a};
         cudaError_t e = cudaLaunchCooperativeKernel((const void*)bfs_kernel, dim3(bfs_grid),
                                                     dim3(kBfsThreads), args, 0, st);
@@ -878,5 +882,49 @@ extern "C" int gsofa_matrix_permute(gsofa_ctx* ctx, const gsofa_matrix* mat, con
         return rc;
     }
     *out = m;
+    return GSOFA_OK;
+}
+
+// The grid barrier's bounded wait, exercised on the device: the BFS kernel
+// runs on a two-vertex graph with no edges, waiting at its first barrier for
+// one block more than the launch has.  Every block's wait runs out after
+// limit_ms; the kernel returns and GSOFA_ERR_TIMEOUT is reported, and the
+// context stays usable.
+extern "C" int gsofa_order_wait_selftest(gsofa_ctx* ctx, double limit_ms) {
+    if (!ctx || !(limit_ms > 0.0) || limit_ms > 2000.0) return GSOFA_ERR_ARG;
+    std::lock_guard<std::recursive_mutex> lk(ctx->mu);
+    if (cudaSetDevice(ctx->device) != cudaSuccess)
+        return set_err(ctx, GSOFA_ERR_CUDA, "cudaSetDevice");
+    cudaStream_t st = ctx->stream;
+    DeviceScratch S(ctx);
+    // rp, trp: 3 zeros (two empty rows); col: 4 ints; part, dist, q0, q1, plo,
+    // H: 2 each; lcnt 4; bar 2 words; err 1
+    int32_t* w = static_cast<int32_t*>(S.get(4 * 64));
+    if (!w) return set_err(ctx, GSOFA_ERR_OOM_BUDGET, "self-test workspace");
+    int32_t h[64];
+    for (int i = 0; i < 64; i++) h[i] = 0;
+    int32_t *rp = w, *col = w + 4, *part = w + 8, *dist = w + 12, *q0 = w + 16, *q1 = w + 20,
+            *plo = w + 24, *H = w + 28, *lcnt = w + 32, *err = w + 40;
+    unsigned* bar = reinterpret_cast<unsigned*>(w + 44);
+    h[12] = 0;   // dist[0] = 0 (the source)
+    h[13] = -1;  // dist[1] unseen
+    h[32] = 1;   // lcnt[0]: one frontier vertex, q0[0] = 0
+    cudaError_t e = cudaMemcpyAsync(w, h, sizeof(h), cudaMemcpyHostToDevice, st);
+    int occ = 0;
+    if (e == cudaSuccess)
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, bfs_kernel, kBfsThreads, 0);
+    if (e != cudaSuccess || occ <= 0) return set_err(ctx, GSOFA_ERR_CUDA, "self-test setup");
+    const int grid = ctx->sm_count * std::min(occ, kBfsBlocksPerSm);
+    Graph g{rp, col, rp, col};
+    BfsArgs a{g, part, plo, dist, q0, q1, lcnt, H, bar, err, 3, (unsigned)grid + 1u,
+              (unsigned long long)(limit_ms * 1e6)};
+    void* args[] = {&a};
+    e = cudaLaunchCooperativeKernel((const void*)bfs_kernel, dim3(grid), dim3(kBfsThreads), args,
+                                    0, st);
+    int32_t herr = 0;
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&herr, err, 4, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "self-test");
+    if (herr) return set_err(ctx, GSOFA_ERR_TIMEOUT, "grid barrier wait gave up (as intended)");
     return GSOFA_OK;
 }

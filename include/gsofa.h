@@ -159,6 +159,11 @@ int gsofa_order_nd(gsofa_ctx* ctx, const gsofa_matrix* mat, int32_t leaf_size, i
  * GSOFA_ERR_ARG). */
 int gsofa_matrix_permute(gsofa_ctx* ctx, const gsofa_matrix* mat, const int32_t* perm,
                          gsofa_matrix** out);
+/* Failure-path self-test of the ordering's grid barrier, whose every wait is
+ * bounded: the BFS kernel is launched waiting for one block more than it
+ * has, each wait gives up after limit_ms (0 < limit_ms <= 2000), and the
+ * call returns GSOFA_ERR_TIMEOUT with the context still usable. */
+int gsofa_order_wait_selftest(gsofa_ctx* ctx, double limit_ms);
 
 /* ---- factorization (replaces the group loop :2965-3218 and its kernels) --- */
 /* Synchronous: returns when the result is complete on the device. */

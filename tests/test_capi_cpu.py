@@ -74,6 +74,7 @@ def test_order_and_permute_reject_null_handles():
     h = ctypes.c_void_p()
     assert L.gsofa_order_nd(None, None, 0, 0, None, ctypes.byref(st)) == _lib.ERR_ARG
     assert L.gsofa_matrix_permute(None, None, None, ctypes.byref(h)) == _lib.ERR_ARG
+    assert L.gsofa_order_wait_selftest(None, 50.0) == _lib.ERR_ARG
     nb = ctypes.c_int64()
     assert L.gsofa_result_supernodal(None, ctypes.byref(nb), None, None, None, None, None, None,
                                      None) == _lib.ERR_ARG

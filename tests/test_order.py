@@ -329,3 +329,25 @@ def test_cli_order_mode(tmp_path):
     ref = _fill(*permuted(b, e, c, perm))
     assert "Final Number of fill-ins detected: %d" % ref in out.stdout, out.stdout
     assert "Ordering (nested dissection on the device)" in out.stdout
+
+
+@pytest.mark.gpu
+def test_grid_barrier_wait_runs_out_and_context_survives(ctx):
+    """The ordering's grid barrier waits with a time limit: launched waiting
+    for one block more than it has, every wait gives up, the kernel returns,
+    the host reports GSOFA_ERR_TIMEOUT, and the context still orders."""
+    import time
+    from gsofatpds_b200 import _lib
+    L = _lib.load()
+    t0 = time.perf_counter()
+    rc = L.gsofa_order_wait_selftest(ctx.handle, 50.0)
+    dt = time.perf_counter() - t0
+    assert rc == _lib.ERR_TIMEOUT, rc
+    assert dt < 5.0, dt
+    assert L.gsofa_order_wait_selftest(ctx.handle, 0.0) == _lib.ERR_ARG
+    b, e, c = _grid2d(30, 30, np.random.default_rng(4))
+    m = ctx.load_csr(b, e, c)
+    perm, _ = ctx.order_nd(m, leaf_size=8)
+    ref, _ = O.order_nd(b, e, c, leaf=8)
+    np.testing.assert_array_equal(perm, ref)
+    m.close()
