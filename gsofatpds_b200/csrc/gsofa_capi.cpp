@@ -5,6 +5,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cmath>
 #include <map>
 #include <cerrno>
 #include <chrono>
@@ -1016,7 +1017,19 @@ int gsofa_autotune(gsofa_ctx* ctx, const gsofa_matrix* mat, gsofa_opts* opts) {
     int lg = 0;
     while ((1ll << (lg + 1)) <= (long long)mat->n) lg++;
     const int deg = (int)((mat->nnz + mat->n / 2) / mat->n);
-    const std::pair<int, int> key(lg, deg);
+    // locality: matrices of one size but different orderings want different
+    // shapes (a renumbered grid is not its banded original)
+    unsigned long long* dsum = reinterpret_cast<unsigned long long*>(
+        reinterpret_cast<char*>(ctx->small) + 96);
+    unsigned long long hsum = 0;
+    cudaError_t ce = cudaMemsetAsync(dsum, 0, 8, ctx->stream);
+    if (ce == cudaSuccess) ce = launch_index_distance(mat->n, mat->rowptr, mat->col, dsum, ctx->stream);
+    if (ce == cudaSuccess) ce = cudaMemcpyAsync(&hsum, dsum, 8, cudaMemcpyDeviceToHost, ctx->stream);
+    if (ce == cudaSuccess) ce = cudaStreamSynchronize(ctx->stream);
+    if (ce != cudaSuccess) return cuda_fail(ctx, ce, "autotune locality");
+    const double rel = mat->nnz > 0 ? (double)hsum / (double)mat->nnz / (double)mat->n : 0.0;
+    const int loc = rel > 1e-9 ? std::max(-60, (int)std::floor(2.0 * std::log2(rel))) : -61;
+    const std::tuple<int, int, int> key(lg, deg, loc);
     auto it = ctx->tuned.find(key);
     if (it != ctx->tuned.end()) {
         opts->threads_per_source = it->second.threads_per_source;

@@ -7,6 +7,7 @@
 #include <map>
 #include <mutex>
 #include <string>
+#include <tuple>
 #include <vector>
 
 #include "../../include/gsofa.h"
@@ -25,8 +26,9 @@ struct gsofa_ctx {
     cudaEvent_t ev0 = nullptr, ev1 = nullptr, evt = nullptr;
     std::recursive_mutex mu;
     std::string err;
-    // autotuner choices per size class (log2 n, mean row length)
-    std::map<std::pair<int, int>, gsofa_opts> tuned;
+    // autotuner choices per class (log2 n, mean row length, locality: half-
+    // octaves of the mean |i - j| of the entries over n)
+    std::map<std::tuple<int, int, int>, gsofa_opts> tuned;
     // pinned staging
     unsigned long long* h_counters = nullptr;  // CNT_SLOTS
     int32_t* h_status = nullptr;

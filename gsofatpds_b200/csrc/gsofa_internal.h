@@ -142,6 +142,9 @@ cudaError_t launch_canonicalize(int32_t n, long long nnz_in, const int32_t* beg,
                                 int32_t* asym, int check_symmetry, void* scan_tmp,
                                 size_t scan_tmp_bytes, int32_t* status, cudaStream_t stream);
 size_t canonicalize_scan_bytes(int32_t n);
+// *sum (zeroed by the caller) += sum over A's entries (v, c) of |v - c|.
+cudaError_t launch_index_distance(int32_t n, const int32_t* rp, const int32_t* col,
+                                  unsigned long long* sum, cudaStream_t stream);
 cudaError_t launch_supernodes(int32_t n, int32_t mss, const int32_t* nz_row_u,
                               const uint32_t* lmask, int8_t* flags,
                               unsigned long long* counters, cudaStream_t stream);

@@ -1283,6 +1283,34 @@ __global__ void transpose_pad_kernel(int32_t n, const int32_t* __restrict__ tcou
     }
 }
 
+// One warp per row: the sum of |v - c| over the row's entries (padding
+// entries repeat v and add nothing).
+__global__ void index_distance_kernel(int32_t n, const int32_t* __restrict__ rp,
+                                      const int32_t* __restrict__ col,
+                                      unsigned long long* sum) {
+    const int lane = threadIdx.x & 31;
+    const long long nw = ((long long)gridDim.x * blockDim.x) >> 5;
+    unsigned long long acc = 0;
+    for (long long v = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5; v < n; v += nw) {
+        const int b = rp[v] & ~3, e = rp[v + 1] & ~3;
+        for (int j = b + lane; j < e; j += 32) {
+            const long long d = (long long)col[j] - v;
+            acc += (unsigned long long)(d < 0 ? -d : d);
+        }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(FULL_MASK, acc, o);
+    if (lane == 0 && acc) atomicAdd(sum, acc);
+}
+
+cudaError_t launch_index_distance(int32_t n, const int32_t* rp, const int32_t* col,
+                                  unsigned long long* sum, cudaStream_t stream) {
+    if (n <= 0) return cudaSuccess;
+    long long g = ((long long)n * 32 + 255) / 256;
+    index_distance_kernel<<<(int)(g > 148 * 16 ? 148 * 16 : g), 256, 0, stream>>>(n, rp, col, sum);
+    return cudaGetLastError();
+}
+
 size_t canonicalize_scan_bytes(int32_t n) {
     size_t bytes = 0;
     cub::DeviceScan::ExclusiveSum(nullptr, bytes, (const int32_t*)nullptr, (int32_t*)nullptr,

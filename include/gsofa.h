@@ -173,8 +173,9 @@ int gsofa_factor_symbolic(gsofa_ctx* ctx, const gsofa_matrix* mat, const gsofa_o
  * chunk_sources, cached_closures, heavy_row) for this matrix on a sample of its work
  * and writes the fastest into *opts (other fields are left as given).
  * Results never depend on these settings.  Choices are cached in the
- * context per size class (log2 n, mean row length), so later calls for
- * similar matrices return at once.  Replaces the reference's fixed sizing
+ * context per class (log2 n, mean row length, and half-octaves of the mean
+ * distance |i - j| of the entries from the diagonal over n, one device pass),
+ * so later calls for similar matrices return at once.  Replaces the reference's fixed sizing
  * (Compute_Src_group, :1031-1048; SPO :1101-1119, :1465-1507). */
 int gsofa_autotune(gsofa_ctx* ctx, const gsofa_matrix* mat, gsofa_opts* opts);
 /* The same search for a batch: each candidate is timed as one persistent
