@@ -27,6 +27,7 @@ PATTERN = 1 << 2
 DIGESTS = 1 << 3
 FORCE_GLOBAL_BITMAP = 1 << 30
 NO_MERGE = 1 << 29
+DEBUG_QUEUE_CAP = 1 << 28
 
 # Every function the header declares (checked by the CPU test-suite).
 EXPORTS = [

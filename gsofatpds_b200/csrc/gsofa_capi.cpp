@@ -340,6 +340,7 @@ int run_factor(gsofa_ctx* ctx, const gsofa_matrix* const* mats, int32_t count,
     L.work_counter = wc;
     L.queue = reinterpret_cast<int32_t*>(ctx->queue);
     L.queue_stride = std::max(nmax, 1);
+    if (o->flags & GSOFA_DEBUG_QUEUE_CAP) L.queue_stride = std::min<long long>(L.queue_stride, 64);
     L.gbitmap = reinterpret_cast<uint32_t*>(ctx->gbitmap);
     L.bitmap_words = cfg.words;
     L.status = dstatus;

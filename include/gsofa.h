@@ -51,6 +51,11 @@ typedef struct gsofa_batch gsofa_batch;
 /* Diagnostic: never reuse the previous source's closure (every source is
  * searched from scratch). */
 #define GSOFA_NO_MERGE (1u << 29)
+/* Fault injection: each CTA's frontier queue holds only 64 entries, so any
+ * search that queues more reports GSOFA_ERR_OVERFLOW (every queue access is
+ * bounds-checked; nothing is written past the bound).  gsofa_factor_symbolic
+ * only. */
+#define GSOFA_DEBUG_QUEUE_CAP (1u << 28)
 
 typedef struct gsofa_opts {
     /* rows per supernode chunk; the reference's max_supernode_size, argv[5]

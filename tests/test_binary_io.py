@@ -108,3 +108,41 @@ def test_binary_load_factors_like_ascii(tmp_path):
                        timeout=300)
     assert r.returncode == 0, r.stderr
     assert "Final Number of fill-ins detected: 980136" in r.stdout
+
+
+def test_malformed_ascii_dat_files_are_io_errors(tmp_path):
+    """The reference's three ASCII files, damaged: too few column ids, a
+    non-numeric token, a missing file, too few row starts.  The parser (the
+    same one gsofa_load_csr_files uses) reports GSOFA_ERR_IO."""
+    from gsofatpds_b200 import GsofaError, convert_dat
+    from gsofatpds_b200 import _lib as C
+    rng = np.random.default_rng(3)
+    n = 40
+    beg, end, col = scrambled_csr(rng, random_pattern(rng, n, 0.1))
+    out = str(tmp_path / "o.gsofacsr")
+    good = _write_dat(str(tmp_path), beg, end, col, n)
+    convert_dat(*good, out)  # the undamaged files convert
+    cases = {}
+    d = tmp_path / "short_csr"
+    d.mkdir()
+    p = _write_dat(str(d), beg, end, col, n)
+    with open(p[2], "w") as f:  # header promises more ids than follow
+        f.write("%d %d\n" % (col.shape[0] + 5, n) + " ".join(map(str, col.tolist())))
+    cases["short_csr"] = p
+    d = tmp_path / "token"
+    d.mkdir()
+    p = _write_dat(str(d), beg, end, col, n)
+    with open(p[0], "w") as f:
+        f.write(" ".join(map(str, beg.tolist()[:-1])) + " x7")
+    cases["token"] = p
+    d = tmp_path / "short_beg"
+    d.mkdir()
+    p = _write_dat(str(d), beg, end, col, n)
+    with open(p[1], "w") as f:
+        f.write(" ".join(map(str, end.tolist()[:-3])))
+    cases["short_end"] = p
+    cases["missing"] = [good[0], good[1], str(tmp_path / "nope.dat")]
+    for name, paths in cases.items():
+        with pytest.raises(GsofaError) as e:
+            convert_dat(*paths, str(tmp_path / ("%s.gsofacsr" % name)))
+        assert e.value.status == C.ERR_IO, name

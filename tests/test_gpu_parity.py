@@ -585,3 +585,21 @@ def test_supernodal_handoff_matches_oracle(ctx, which):
     assert res.supernodal()["lrows"].shape == got["lrows"].shape  # cached, same answer
     res.close()
     m.close()
+
+
+def test_forced_queue_overflow_is_an_error_and_the_context_survives(ctx):
+    """Fault injection (GSOFA_DEBUG_QUEUE_CAP): 64-entry frontier queues make
+    BC's long searches overflow; the bounds-checked queue turns that into
+    GSOFA_ERR_OVERFLOW, and the next plain factorization is exact."""
+    from gsofatpds_b200 import GsofaError
+    from gsofatpds_b200 import _lib as C
+    z = load_bc()
+    m = ctx.load_csr(z["beg"], z["end"], z["col"])
+    with pytest.raises(GsofaError) as e:
+        ctx.factor(m, debug_queue_cap=True)
+    assert e.value.status == C.ERR_OVERFLOW
+    r = ctx.factor(m)
+    assert r.counts["fill_count"] == 980136
+    np.testing.assert_array_equal(r.row_counts()["nnz_u_row"], z["nnzU"])
+    r.close()
+    m.close()
