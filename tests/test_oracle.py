@@ -165,3 +165,28 @@ def test_digest_definitions(seed):
         L = r["Lcols"][r["Lptr"][s]:r["Lptr"][s + 1]]
         dl = sum(O.mix64(int(c)) for c in L) & M
         assert dl == int(r["digL"][s]), (seed, s)
+
+
+@pytest.mark.parametrize("seed", range(8))
+def test_supernodal_form_reference_equals_elimination(seed):
+    """The restatement the GPU handoff test compares against
+    (`_supernodal_reference`: per-block unions from the oracle's patterns)
+    equals the same unions read off symbolic Gaussian elimination."""
+    from tests.test_gpu_parity import _supernodal_reference
+    rng = np.random.default_rng(300 + seed)
+    n = int(rng.integers(2, 60))
+    pat = random_pattern(rng, n, float(rng.uniform(0.02, 0.12)))
+    beg, end, col = scrambled_csr(rng, pat)
+    r = O.rows(beg, end, col, pattern=True)
+    mss = [4, 8, 128][seed % 3]
+    _, flags = O.supernodes(r["nzU_ref"], r["lback"], mss)
+    got = _supernodal_reference(n, r, flags)
+    F = symbolic_elimination(n, pat)
+    starts = list(np.nonzero(flags)[0]) + [n]
+    np.testing.assert_array_equal(got["block_start"], starts)
+    for k in range(len(starts) - 1):
+        f, l = starts[k], starts[k + 1]
+        rows = sorted({i for i in range(l, n) for c in range(f, l) if F[i, c]})
+        cols = sorted({j for j in range(l, n) for i in range(f, l) if F[i, j]})
+        assert got["lrows"][got["lptr"][k]:got["lptr"][k + 1]] == rows, (seed, k)
+        assert got["ucols"][got["uptr"][k]:got["uptr"][k + 1]] == cols, (seed, k)
