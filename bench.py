@@ -173,6 +173,11 @@ def run_reference(args, rank, world):
     as CUDA kernels; its GPU build is not run here)."""
     if rank != 0:
         return
+    if args.workload not in ("circuit_like", "random_extra", "grid3d_64", "circuit_like_100k"):
+        print(json.dumps({"impl": "reference", "unavailable": "the reference has no counterpart "
+                          "of the %s workload (it factors one matrix per run)" % args.workload}),
+              flush=True)
+        return
     (n, rp, col), mss = make_workload(args.workload)
     per_step = max(2.0, min(20.0, 60.0 / max(args.steps + args.warmup, 1)))
     for i in range(args.warmup):
