@@ -236,9 +236,9 @@ int build(gsofa_result* r) {
     long long nl = 0, nu = 0;
     int rc = one_side(ctx, S, n, nb, r->lptr, r->lrows, blk, start, lp, &r->sn_lrows, &nl);
     if (rc) return rc;
+    r->sn_nl = nl;  // recorded at once: a failure below frees it with its size
     rc = one_side(ctx, S, n, nb, r->uptr, r->ucols, blk, start, up, &r->sn_ucols, &nu);
     if (rc) return rc;
-    r->sn_nl = nl;
     r->sn_nu = nu;
     if (cudaStreamSynchronize(st) != cudaSuccess)
         return set_err(ctx, GSOFA_ERR_CUDA, "supernodal form");
