@@ -105,6 +105,7 @@ static int one_row(or_ws* w, int32_t n, const int32_t* beg, const int32_t* end,
                    uint64_t* e_alg, uint64_t* v_alg, uint32_t* lback,
                    const int64_t* Loff, int32_t* Lcols,
                    const int64_t* Uoff, int32_t* Ucols) {
+    (void)n;  /* the workspace was sized for n by ws_init */
     uint32_t* lab = w->lab;
     w->ntouched = 0;
     w->plen = 0;
