@@ -49,6 +49,7 @@ class Context:
 
     @property
     def handle(self):
+        """The gsofa_ctx* handle (for calls through gsofatpds_b200._lib)."""
         return self._h
 
     def set_stream(self, stream_ptr):
@@ -57,6 +58,7 @@ class Context:
         self._check(self._L.gsofa_set_stream(self._h, ctypes.c_void_p(stream_ptr or 0)), "set_stream")
 
     def memory_used(self):
+        """Device bytes the context holds now (matrices, results, workspace)."""
         v = ctypes.c_size_t()
         self._check(self._L.gsofa_memory_used(self._h, ctypes.byref(v)), "memory_used")
         return v.value
@@ -75,6 +77,7 @@ class Context:
         return Matrix(self, h)
 
     def load_rowptr(self, rowptr, col):
+        """load_csr for contiguous rows: row v is col[rowptr[v]:rowptr[v+1]]."""
         rowptr = np.ascontiguousarray(rowptr, dtype=np.int32)
         return self.load_csr(rowptr[:-1], rowptr[1:], col)
 
@@ -86,6 +89,7 @@ class Context:
         return Matrix(self, h)
 
     def load_files(self, beg_file, end_file, csr_file):
+        """The reference's three ASCII files (colbeg, colend, csr) -> matrix."""
         h = ctypes.c_void_p()
         self._check(self._L.gsofa_load_csr_files(self._h, beg_file.encode(), end_file.encode(),
                                                  csr_file.encode(), ctypes.byref(h)), "load_files")
@@ -96,6 +100,8 @@ class Context:
              supernodes=True, digests=True, l_row_stats=False, pattern=False,
              bu_alpha=0, bu_beta=0, heavy_row=0, bu_min_source=0, chunk_sources=0,
              merge=True, cached_closures=0, global_bitmap=False, debug_queue_cap=False):
+        """A gsofa_opts from keyword arguments (0 = library default); the
+        launch-shape options change speed only, never results."""
         o = C.Opts()
         o.cached_closures = int(cached_closures)
         o.chunk_sources = int(chunk_sources)
@@ -153,6 +159,8 @@ class Context:
         return Matrix(self, h)
 
     def factor(self, mat, **kw):
+        """gsofa_factor_symbolic: the fill structure of `mat` (a Result);
+        keyword arguments as for opts()."""
         o = self.opts(**kw)
         h = ctypes.c_void_p()
         self._check(self._L.gsofa_factor_symbolic(self._h, mat.handle, ctypes.byref(o),
@@ -168,6 +176,7 @@ class Context:
         return Server(self, max_n, budget_bytes, **kw)
 
     def factor_batch(self, mats, **kw):
+        """All `mats` in one persistent launch; one Result per matrix."""
         o = self.opts(**kw)
         k = len(mats)
         arr = (ctypes.c_void_p * max(k, 1))(*[m.handle for m in mats])
@@ -177,6 +186,7 @@ class Context:
         return [Result(self, ctypes.c_void_p(outs[i])) for i in range(k)]
 
     def close(self):
+        """Releases the context and everything it holds on the device."""
         if getattr(self, "_h", None):
             self._L.gsofa_destroy(self._h)
             self._h = None
@@ -204,10 +214,12 @@ class Batch:
         self._h = h
 
     def run(self):
+        """Replays the captured launch; results are refreshed in place."""
         self.ctx._check(self.ctx._L.gsofa_batch_run(self._h), "batch_run")
         return self
 
     def result(self, i):
+        """The i-th matrix's Result (owned by the batch)."""
         h = ctypes.c_void_p()
         self.ctx._check(self.ctx._L.gsofa_batch_result(self._h, int(i), ctypes.byref(h)), "batch_result")
         return Result(self.ctx, h, owned=False)
@@ -252,6 +264,7 @@ class Server:
         return t.value
 
     def submit_rowptr(self, rowptr, col):
+        """submit() for contiguous rows (rowptr of n+1 entries)."""
         rowptr = np.asarray(rowptr)
         return self.submit(rowptr[:-1], rowptr[1:], col)
 
@@ -275,6 +288,7 @@ class Server:
         return self._finish(ticket, rc, h)
 
     def info(self, ticket):
+        """A ticket's times (submit, admit, publish, done; ms), footprint and status."""
         i = C.TicketInfo()
         rc = self._L.gsofa_server_ticket_info(self._h, int(ticket), ctypes.byref(i))
         if rc != C.OK:
@@ -282,6 +296,7 @@ class Server:
         return {f: getattr(i, f) for f, _ in C.TicketInfo._fields_}
 
     def stats(self):
+        """The loop's counters: requests, launches, memory in use and peak."""
         st = C.ServerStats()
         rc = self._L.gsofa_server_get_stats(self._h, ctypes.byref(st))
         if rc != C.OK:
@@ -332,6 +347,8 @@ class Result:
         self.n = c.n
 
     def row_counts(self, l_rows=False):
+        """Per-row arrays: |U row|, the reference's nz_row_U, |L column| and,
+        with l_rows (needs the l_row_stats option), |L row|."""
         n = self.n
         u = np.zeros(n, np.int32)
         nzu = np.zeros(n, np.int32)
@@ -345,6 +362,7 @@ class Result:
         return out
 
     def digests(self, l_rows=False):
+        """64-bit column-set digests per U row and L column (and L row)."""
         n = self.n
         du = np.zeros(n, np.uint64)
         dl = np.zeros(n, np.uint64)
@@ -357,6 +375,7 @@ class Result:
         return out
 
     def supernodes(self):
+        """(flags int8[n], boundaries): non-zero flags start a supernode."""
         flags = np.zeros(self.n, np.int8)
         cnt = ctypes.c_int64()
         self.ctx._check(self.ctx._L.gsofa_result_supernodes(self._h, _ptr(flags), None, 0,
@@ -364,6 +383,7 @@ class Result:
         return flags, np.nonzero(flags)[0].astype(np.int32)
 
     def lmask(self):
+        """(n, 4) uint32: bit j of column f's mask is L(f+1+j, f) != 0."""
         m = np.zeros((self.n, 4), np.uint32)
         self.ctx._check(self.ctx._L.gsofa_result_lmask(self._h, _ptr(m)), "lmask")
         return m
