@@ -72,6 +72,26 @@ def read_peaks():
     return 6650.0, "fallback"
 
 
+def roofline_entry(edges, vertices_alg, n, kernel_ms, peak, peak_kind, traffic):
+    """The line's roofline object for the traversal kernel.  `achieved` is
+    the algorithmic bytes (8 E_alg + 16 V_alg + 4 W_out) per second of the
+    kernel; closure reuse makes it exceed the HBM peak.  `traffic` is the
+    DRAM bytes one launch really moves (ncu), and traffic_achieved /
+    traffic_frac are that rate against the same peak."""
+    w_out = 11 * n  # nnz_u, nz_row_u, nnz_lc, 2 digests (u64), 128-bit L-mask per row
+    bytes_alg = 8 * edges + 16 * vertices_alg + 4 * w_out
+    achieved = bytes_alg / (kernel_ms / 1e3) / 1e9
+    roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+            "frac": achieved / peak, "traffic": traffic,
+            "peak_kind": peak_kind + " (MEASURED_PEAKS hbm_gbs)",
+            "kernel": "traverse_kernel", "kernel_ms": kernel_ms,
+            "bytes_alg": bytes_alg}
+    if traffic:
+        roof["traffic_achieved"] = traffic / (kernel_ms / 1e3) / 1e9
+        roof["traffic_frac"] = roof["traffic_achieved"] / peak
+    return roof
+
+
 def read_traffic(workload):
     """dram bytes per traversal launch from the committed ncu summary."""
     p = os.path.join(ROOT, "profiles", "traverse_%s.md" % workload)
@@ -758,15 +778,8 @@ def main():
     if rank == 0:
         peak, peak_kind = read_peaks()
         trav = float(np.mean(trav_ms))
-        w_out = 11 * n  # nnz_u, nz_row_u, nnz_lc, 2 digests (u64), 128-bit L-mask per row
-        bytes_alg = 8 * edges + 16 * counts["vertices_alg"] + 4 * w_out
-        achieved = bytes_alg / (trav / 1e3) / 1e9
-        traffic = read_traffic(args.workload)
-        roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                "frac": achieved / peak, "traffic": traffic,
-                "peak_kind": peak_kind + " (MEASURED_PEAKS hbm_gbs)",
-                "kernel": "traverse_kernel", "kernel_ms": trav,
-                "bytes_alg": bytes_alg}
+        roof = roofline_entry(edges, counts["vertices_alg"], n, trav, peak, peak_kind,
+                              read_traffic(args.workload))
         line = {"metric": "fill_path_gteps", "value": value, "unit": "GTEPS", "n_gpus": world,
                 "steps": args.steps, "warmup": args.warmup,
                 "ms_per_step": max_ms / args.steps, "higher_is_better": True,

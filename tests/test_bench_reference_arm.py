@@ -30,3 +30,17 @@ def test_reference_arm_without_a_counterpart_is_unavailable():
     assert out.returncode == 0, out.stderr[-2000:]
     line = json.loads([x for x in out.stdout.splitlines() if x.startswith("{")][-1])
     assert line["impl"] == "reference" and "unavailable" in line
+
+
+def test_roofline_entry():
+    sys.path.insert(0, ROOT)
+    import bench
+    # config 2's numbers: E_alg, V_alg, n, kernel ms, measured peak, ncu bytes per launch
+    r = bench.roofline_entry(1316542257033, 148212479438, 659033, 871.76, 6456.2, "measured",
+                             548526653696.0)
+    assert r["bytes_alg"] == 8 * 1316542257033 + 16 * 148212479438 + 4 * 11 * 659033
+    assert abs(r["frac"] - r["achieved"] / 6456.2) < 1e-12
+    assert abs(r["traffic_achieved"] - 548526653696.0 / 0.87176 / 1e9) < 1e-6
+    assert 0.09 < r["traffic_frac"] < 0.11
+    r0 = bench.roofline_entry(10, 1, 5, 1.0, 100.0, "fallback", None)
+    assert r0["traffic"] is None and "traffic_frac" not in r0
