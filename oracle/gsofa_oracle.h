@@ -84,6 +84,12 @@ int64_t or_supernodes(int32_t n, const int32_t* nzU, const uint32_t* lback,
 int or_order_nd(int32_t n, const int32_t* beg, const int32_t* end, const int32_t* col,
                 int32_t leaf, int32_t max_rounds, int32_t* perm, int64_t* stats);
 
+/* The hybrid rule (gsofa_order_hybrid_oracle.c): or_order_nd with, at every
+ * split, a deterministic multilevel separator computed too and the smaller
+ * of the two used.  Same outputs as or_order_nd (no round cap). */
+int or_order_hybrid(int32_t n, const int32_t* beg, const int32_t* end, const int32_t* col,
+                    int32_t leaf, int32_t* perm, int64_t* stats);
+
 /* Parse the reference's ASCII files (csr: "E N" then E ids; beg/end: n ids).
  * Allocates *beg,*end,*col with malloc; caller frees with or_free.
  * Returns 0 or -1. */

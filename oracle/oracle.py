@@ -40,6 +40,8 @@ def lib():
                                                           ctypes.POINTER(ctypes.c_int64)] + \
             [ctypes.POINTER(ctypes.POINTER(ctypes.c_int32))] * 3
         L.or_free.argtypes = [vp]
+        L.or_order_hybrid.restype = ctypes.c_int
+        L.or_order_hybrid.argtypes = [ctypes.c_int32, vp, vp, vp, ctypes.c_int32, vp, vp]
         L.or_order_nd.restype = ctypes.c_int
         L.or_order_nd.argtypes = [ctypes.c_int32, vp, vp, vp, ctypes.c_int32, ctypes.c_int32, vp,
                                   vp]
@@ -124,6 +126,22 @@ def order_nd(beg, end, col, leaf=32, max_rounds=512):
     stats = np.zeros(4, np.int64)
     rc = lib().or_order_nd(n, _p(b), _p(e), _p(c), int(leaf), int(max_rounds), _p(perm),
                            _p(stats))
+    if rc != 0:
+        raise ValueError("oracle: bad ordering arguments")
+    return perm[:n], tuple(int(x) for x in stats)
+
+
+def order_hybrid(beg, end, col, leaf=32):
+    """The hybrid nested-dissection rule (gsofa_order_hybrid_oracle.c):
+    level-set ND where, at each split, a multilevel separator is also
+    computed and the smaller one used.  Returns (perm, stats) like order_nd."""
+    b = np.ascontiguousarray(beg, dtype=np.int32)
+    e = np.ascontiguousarray(end, dtype=np.int32)
+    c = np.ascontiguousarray(col, dtype=np.int32)
+    n = b.shape[0]
+    perm = np.zeros(max(n, 1), np.int32)
+    stats = np.zeros(4, np.int64)
+    rc = lib().or_order_hybrid(n, _p(b), _p(e), _p(c), int(leaf), _p(perm), _p(stats))
     if rc != 0:
         raise ValueError("oracle: bad ordering arguments")
     return perm[:n], tuple(int(x) for x in stats)

@@ -351,3 +351,45 @@ def test_grid_barrier_wait_runs_out_and_context_survives(ctx):
     ref, _ = O.order_nd(b, e, c, leaf=8)
     np.testing.assert_array_equal(perm, ref)
     m.close()
+
+
+# ---- the hybrid rule (oracle only; no device counterpart yet) --------------------
+
+@pytest.mark.parametrize("seed", range(12))
+def test_hybrid_oracle_is_a_deterministic_permutation(seed):
+    rng = np.random.default_rng(700 + seed)
+    n = int(rng.integers(1, 900))
+    dens = float(rng.uniform(0.0, 0.02))
+    rows = [[int(j) for j in np.nonzero(rng.random(n) < dens)[0]] for _ in range(n)]
+    b, e, c = _csr(rows)
+    leaf = int(rng.choice([1, 8, 32]))
+    p1, s1 = O.order_hybrid(b, e, c, leaf=leaf)
+    assert sorted(p1.tolist()) == list(range(n))
+    p2, s2 = O.order_hybrid(b, e, c, leaf=leaf)
+    np.testing.assert_array_equal(p1, p2)
+    assert s1 == s2
+
+
+def test_hybrid_equals_level_set_when_level_sets_win():
+    # a path: the level-set separator is one vertex, which no other can beat
+    for n in (7, 50, 301):
+        b, e, c = _path(n)
+        ph, sh = O.order_hybrid(b, e, c, leaf=1)
+        pl, sl = O.order_nd(b, e, c, leaf=1)
+        np.testing.assert_array_equal(ph, pl)
+        assert sh == sl
+
+
+def test_hybrid_cuts_circuit_like_fill():
+    _, rp, col = gen_circuit(12000)
+    b, e = rp[:-1], rp[1:]
+    pl, _ = O.order_nd(b, e, col, leaf=32)
+    ph, _ = O.order_hybrid(b, e, col, leaf=32)
+    f_l = _fill(*permuted(b, e, col, pl))
+    f_h = _fill(*permuted(b, e, col, ph))
+    assert f_h < f_l, (f_h, f_l)
+
+
+def gen_circuit(n):
+    from gsofatpds_b200 import gen
+    return gen.circuit_like(n=n, target_nnz=int(5830000 * n / 659033), seed=2)
