@@ -28,7 +28,7 @@
  *              other side) - (to its own side); a vertex with positive gain
  *              larger than every neighbour's (ties: the smaller id wins) is
  *              a candidate; candidates are taken in increasing id, each
- *              moved only if side 0's weight stays within 45..55 % of the
+ *              moved only if side 0's weight stays within 40..60 % of the
  *              total (the others are skipped).
  *   separator  the boundary vertices (with a neighbour on the other side) of
  *              the side that has fewer of them (ties: side 0); A = side 0
@@ -251,7 +251,7 @@ static void hg_refine(const hg* g, int* side) {
             }
             if (!best) continue;
             const int64_t nw0 = side[v] ? w0 + g->vw[v] : w0 - g->vw[v];
-            if (nw0 * 100 < total * 45 || nw0 * 100 > total * 55) continue;
+            if (nw0 * 100 < total * 40 || nw0 * 100 > total * 60) continue;
             side[v] ^= 1;
             w0 = nw0;
             moved++;
