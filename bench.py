@@ -213,7 +213,8 @@ def run_reference(args, rank, world):
     line = {"impl": "reference", "metric": "fill_path_gteps", "value": v, "unit": "GTEPS",
             "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int32",
-            "data": "synthetic", "config": {"workload": WORKLOADS[args.workload], "mss": mss},
+            "data": "synthetic", "config": {"workload": WORKLOADS[args.workload], "n": n,
+                                            "nnz": int(rp[-1]), "mss": mss},
             "cpu_baseline": cb,
             "e2e": {"value": v, "unit": "GTEPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)

@@ -28,6 +28,7 @@ DIGESTS = 1 << 3
 FORCE_GLOBAL_BITMAP = 1 << 30
 NO_MERGE = 1 << 29
 DEBUG_QUEUE_CAP = 1 << 28
+NO_CHAIN = 1 << 27
 
 # Every function the header declares (checked by the CPU test-suite).
 EXPORTS = [
@@ -68,7 +69,8 @@ class Counts(ctypes.Structure):
                 ("nnz_u", ctypes.c_uint64), ("nnz_lu", ctypes.c_uint64),
                 ("n_supernodes", ctypes.c_int64), ("edges_alg", ctypes.c_uint64),
                 ("vertices_alg", ctypes.c_uint64), ("edges_traversed", ctypes.c_uint64),
-                ("ms_device", ctypes.c_double), ("ms_traverse", ctypes.c_double)]
+                ("ms_device", ctypes.c_double), ("ms_traverse", ctypes.c_double),
+                ("sources_chained", ctypes.c_uint64)]
 
 
 class OrderStats(ctypes.Structure):

@@ -99,7 +99,8 @@ class Context:
     def opts(max_supernode_size=128, threads_per_source=0, sources_in_flight=0,
              supernodes=True, digests=True, l_row_stats=False, pattern=False,
              bu_alpha=0, bu_beta=0, heavy_row=0, bu_min_source=0, chunk_sources=0,
-             merge=True, cached_closures=0, global_bitmap=False, debug_queue_cap=False):
+             merge=True, cached_closures=0, global_bitmap=False, debug_queue_cap=False,
+             chain=True):
         """A gsofa_opts from keyword arguments (0 = library default); the
         launch-shape options change speed only, never results."""
         o = C.Opts()
@@ -115,7 +116,7 @@ class Context:
         o.flags = ((C.SUPERNODES if supernodes else 0) | (C.DIGESTS if digests else 0) |
                    (C.L_ROW_STATS if l_row_stats else 0) | (C.PATTERN if pattern else 0) |
                    (0 if merge else C.NO_MERGE) | (C.FORCE_GLOBAL_BITMAP if global_bitmap else 0) |
-                   (C.DEBUG_QUEUE_CAP if debug_queue_cap else 0))
+                   (C.DEBUG_QUEUE_CAP if debug_queue_cap else 0) | (0 if chain else C.NO_CHAIN))
         return o
 
     def autotune(self, mat, **kw):

@@ -150,11 +150,12 @@ int plan_launch(gsofa_ctx* ctx, int32_t nmax, const gsofa_opts* o, LaunchCfg* c)
 }
 
 int check_status(gsofa_ctx* ctx) {
-    int32_t s = *ctx->h_status;
-    if (s & DEV_ERR_COL_RANGE) return set_err(ctx, GSOFA_ERR_ARG, "column id outside [0, n)");
-    if (s & DEV_ERR_ROW_RANGE) return set_err(ctx, GSOFA_ERR_ARG, "row interval outside [0, nnz)");
-    if (s & DEV_ERR_QUEUE) return set_err(ctx, GSOFA_ERR_OVERFLOW, "traversal queue bound exceeded");
-    return GSOFA_OK;
+    const int32_t s = *ctx->h_status;
+    const int code = device_status_code(s);
+    if (code == GSOFA_OK) return GSOFA_OK;
+    if (s & DEV_ERR_COL_RANGE) return set_err(ctx, code, "column id outside [0, n)");
+    if (s & DEV_ERR_ROW_RANGE) return set_err(ctx, code, "row interval outside [0, nnz)");
+    return set_err(ctx, code, "traversal queue bound exceeded");
 }
 
 int32_t* work_counter_status(gsofa_ctx* ctx, unsigned long long** wc) {
@@ -174,11 +175,11 @@ void result_free(gsofa_result* r) {
 }
 
 // Layout of a result arena: the per-row arrays of an n-row matrix.
-static size_t result_layout(int32_t n, uint32_t flags, size_t off[10]) {
+static size_t result_layout(int32_t n, uint32_t flags, size_t off[11]) {
     const size_t N = (size_t)std::max(n, 1);
     const bool dig = flags & GSOFA_DIGESTS;
     const bool lrow = flags & GSOFA_L_ROW_STATS;
-    size_t sz[10];
+    size_t sz[11];
     sz[0] = 4 * N;                       // nnz_u
     sz[1] = 4 * N;                       // nz_row_u
     sz[2] = dig ? 8 * N : 0;             // dig_u
@@ -189,8 +190,9 @@ static size_t result_layout(int32_t n, uint32_t flags, size_t off[10]) {
     sz[7] = lrow ? 8 * N : 0;            // dig_lr
     sz[8] = N;                           // supernode flags
     sz[9] = 8 * CNT_SLOTS;               // counters
+    sz[10] = 2 * N;                      // link (chained starts)
     size_t total = 0;
-    for (int i = 0; i < 10; i++) {
+    for (int i = 0; i < 11; i++) {
         off[i] = total;
         total += align256(sz[i]);
     }
@@ -198,7 +200,7 @@ static size_t result_layout(int32_t n, uint32_t flags, size_t off[10]) {
 }
 
 size_t result_bytes(int32_t n, uint32_t flags) {
-    size_t off[10];
+    size_t off[11];
     return result_layout(n, flags, off);
 }
 
@@ -214,7 +216,7 @@ int result_alloc_on(gsofa_ctx* ctx, int32_t n, uint32_t flags, int32_t mss, cuda
     const size_t N = (size_t)std::max(n, 1);
     const bool dig = flags & GSOFA_DIGESTS;
     const bool lrow = flags & GSOFA_L_ROW_STATS;
-    size_t off[10];
+    size_t off[11];
     const size_t total = result_layout(n, flags, off);
     int rc = dev_alloc_on(ctx, total, &r->arena, stream);
     if (rc) {
@@ -233,6 +235,7 @@ int result_alloc_on(gsofa_ctx* ctx, int32_t n, uint32_t flags, int32_t mss, cuda
     r->dig_lr = lrow ? reinterpret_cast<uint64_t*>(b + off[7]) : nullptr;
     r->sflags = reinterpret_cast<int8_t*>(b + off[8]);
     r->counters = reinterpret_cast<unsigned long long*>(b + off[9]);
+    r->link = reinterpret_cast<uint8_t*>(b + off[10]);
     // zero the scatter targets, the counters and the flags
     cudaError_t e = cudaSuccess;
     if (lrow) {
@@ -241,6 +244,7 @@ int result_alloc_on(gsofa_ctx* ctx, int32_t n, uint32_t flags, int32_t mss, cuda
     }
     if (e == cudaSuccess) e = cudaMemsetAsync(r->counters, 0, 8 * CNT_SLOTS, stream);
     if (e == cudaSuccess) e = cudaMemsetAsync(r->sflags, 0, N, stream);
+    if (e == cudaSuccess) e = cudaMemsetAsync(r->link, 0, 2 * N, stream);
     if (e != cudaSuccess) {
         dev_free_on(ctx, r->arena, r->bytes, stream);
         delete r;
@@ -280,6 +284,7 @@ MatDesc make_desc(const gsofa_matrix* m, const gsofa_result* r, long long base) 
     d.ucols = r->ucols;
     d.lptr = r->lptr;
     d.lrows = r->lrows;
+    d.link = r->link;
     d.item_base = base;
     return d;
 }
@@ -350,6 +355,7 @@ int run_factor(gsofa_ctx* ctx, const gsofa_matrix* const* mats, int32_t count,
     L.bu_min_src = o->bu_min_source > 0 ? o->bu_min_source : kBuMinSource;
     L.gprev = reinterpret_cast<uint32_t*>(ctx->gprev);
     L.merge = merge ? 1 : 0;
+    L.chain = merge && !(o->flags & GSOFA_NO_CHAIN) ? 1 : 0;
     L.ring = ring;
     L.chunk = (int)chunk;
     L.heavy_len = o->heavy_row > 0 ? ((o->heavy_row + 3) & ~3) : kDefaultHeavyRow;
@@ -432,6 +438,7 @@ int run_factor(gsofa_ctx* ctx, const gsofa_matrix* const* mats, int32_t count,
         k.edges_alg = c[CNT_EDGES_ALG];
         k.vertices_alg = c[CNT_VERTS_ALG];
         k.edges_traversed = c[CNT_EDGES_TRAV];
+        k.sources_chained = c[CNT_CHAINED];
         k.ms_device = (double)ms;  // for a batch: the whole launch
         k.ms_traverse = (double)ms_trav;
     }
@@ -1199,6 +1206,7 @@ int gsofa_batch_create(gsofa_ctx* ctx, const gsofa_matrix* const* mats, int32_t 
     L.gprev = dring;
     L.chunk = (int)chunk;
     L.merge = merge ? 1 : 0;
+    L.chain = merge && !(o.flags & GSOFA_NO_CHAIN) ? 1 : 0;
     L.ring = ring;
     L.sample_stride = 1;
 
@@ -1258,6 +1266,7 @@ int gsofa_batch_run(gsofa_batch* b) {
         k.edges_alg = c[CNT_EDGES_ALG];
         k.vertices_alg = c[CNT_VERTS_ALG];
         k.edges_traversed = c[CNT_EDGES_TRAV];
+        k.sources_chained = c[CNT_CHAINED];
         k.ms_device = (double)ms;  // the whole batch (one graph launch)
         k.ms_traverse = (double)ms;
     }

@@ -76,6 +76,7 @@ struct gsofa_result {
     uint64_t* dig_lr = nullptr;
     int8_t* sflags = nullptr;
     unsigned long long* counters = nullptr;
+    uint8_t* link = nullptr;  // 2n: chained-start links between the directions
     // pattern (separate allocation, only with GSOFA_PATTERN)
     void* parena = nullptr;
     size_t pbytes = 0;

@@ -3,6 +3,8 @@
 #include <cstdint>
 #include <cuda_runtime.h>
 
+#include "../../include/gsofa.h"
+
 namespace gsofa {
 
 // Device-side error word bits (read back by the host after every launch).
@@ -11,6 +13,15 @@ enum : int32_t {
     DEV_ERR_ROW_RANGE = 2,   // a row interval outside [0, nnz) or begin > end
     DEV_ERR_QUEUE = 4,       // a traversal queue write past its bound
 };
+
+// The status code a device error word stands for: row or column ids out of
+// range are the caller's input (GSOFA_ERR_ARG), a queue write past its bound
+// is GSOFA_ERR_OVERFLOW; no bit set is GSOFA_OK.
+inline int device_status_code(int32_t s) {
+    if (s & (DEV_ERR_COL_RANGE | DEV_ERR_ROW_RANGE)) return GSOFA_ERR_ARG;
+    if (s & DEV_ERR_QUEUE) return GSOFA_ERR_OVERFLOW;
+    return GSOFA_OK;
+}
 
 // Counter slots of MatOut::counters.
 enum : int {
@@ -21,6 +32,7 @@ enum : int {
     CNT_NSUP = 4,
     CNT_NNZ_U = 5,
     CNT_NNZ_L = 6,
+    CNT_CHAINED = 7,   // source searches that started from the previous source's closure
     CNT_SLOTS = 8,
 };
 
@@ -55,6 +67,11 @@ struct MatDesc {
     int32_t* ucols;
     const int64_t* lptr;        // pattern pass: L column pointers (n+1) or null
     int32_t* lrows;
+    // 2n bytes or null: link[2 s + d] is 0 until the direction-d search of
+    // source s has finished, then 1 + (s+1 is in its closure): for d = 0 that
+    // bit is U(s, s+1), for d = 1 it is L(s+1, s).  The search of source s+1
+    // in the other direction reads it (see traverse_kernel: chained starts)
+    uint8_t* link;
     long long item_base;        // first work item of this matrix
     // serving only (zero elsewhere)
     long long n_items;          // work items of this request
@@ -109,6 +126,7 @@ struct TraverseLaunch {
     uint32_t* gprev;            // grid * ring * bitmap_words: each CTA's recent closures
     int chunk;                  // consecutive sources per work item
     int merge;                  // 1: reuse the closures of reached cached sources
+    int chain;                  // 1: start a source from the previous source's closure when it is known to hold
     int ring;                   // cached closures per CTA (power of 2, <= 64)
     long long sample_stride;    // > 1: process only every stride-th item (autotuner timing)
     long long bitmap_words;     // words per bitmap (covers max n + padding)

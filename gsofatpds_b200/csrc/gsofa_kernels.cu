@@ -92,6 +92,22 @@ __device__ __forceinline__ int row_degree(const int32_t* rp, int v) {
 // Ring slot masks: one bit per closure-ring slot (up to 64 slots).
 typedef unsigned long long rmask_t;
 
+// Chained starts.  When source s-1 lies in R(s) -- for a U row that is
+// L(s, s-1) != 0, for an L column U(s-1, s) != 0 -- the whole closure of s-1
+// belongs to the closure of s and every vertex of it is already expanded, so
+// the search of s starts from the bitmap s-1 left behind instead of an empty
+// one and expands only what is new.  Whether it holds is known before s
+// starts: symmetric patterns read it from s-1's own bitmap (bit s), the other
+// patterns from the other direction's search of s-1 (MatDesc::link), when
+// that one has finished already.  With the old bits in place, a first
+// occurrence of an id > s in the source row can no longer be told from a
+// fresh bit, so chained starts count the distinct ids of that row through a
+// small set in shared memory; only rows of up to kChainMaxRow entries chain.
+constexpr int kHsetCap = 256;
+constexpr int kChainMaxRow = 128;
+// the set, one per CTA (static shared memory of every kernel that uses it)
+__shared__ int chain_hset[kHsetCap];
+
 template <int BLOCK>
 struct TraverseSmem {
     typedef cub::BlockScan<int, BLOCK> Scan;
@@ -111,6 +127,7 @@ struct TraverseSmem {
     int sym;              // the current item's matrix has a symmetric pattern
     int ring_lo[64];      // per ring slot: the words its closure occupies
     int ring_hi[64];
+    int chain;            // the next source starts from this source's bitmap
 };
 
 // Bitmap words of a matrix of order n: n bits plus zero padding read by the
@@ -142,6 +159,9 @@ struct Src {
     rmask_t pending;                  // cached sources a merge set, not yet merged (slots)
     int* abort_flag;
     rmask_t* reached;                 // slots of cached sources first reached this level
+    int qmark;                        // queue entries from here on were queued after the
+                                      // last merge: none lies in the top merged closure
+    bool chained;                     // started from the previous source's closure
 };
 
 // The cached source held in ring slot j.
@@ -169,6 +189,21 @@ __device__ __forceinline__ int top_slot(const Src& S, rmask_t mask) {
     return -1;
 }
 
+// Inserts w (>= 0) into the open-addressing set h of kHsetCap slots (-1 =
+// empty); returns 1 when w was not there.  Holds at most kChainMaxRow keys,
+// so a free slot or w itself is always found.
+__device__ __forceinline__ uint32_t hset_insert(int w) {
+    int* const h = chain_hset;
+    unsigned k = ((unsigned)w * 0x9E3779B1u) >> 24;  // 8 bits: kHsetCap = 256
+    for (int p = 0; p < kHsetCap; p++) {
+        const int old = atomicCAS(h + k, -1, w);
+        if (old == -1) return 1u;
+        if (old == w) return 0u;
+        k = (k + 1) & (kHsetCap - 1);
+    }
+    return 0u;
+}
+
 // Top-down visit of edge v -> w.  Returns true when w is a new vertex < src
 // to queue.  w == src (also the sentinel of idle lanes and the padding of the
 // source's row) is a no-op.  raw / orig count the source row's entries > src
@@ -187,7 +222,8 @@ __device__ __forceinline__ bool td_edge(const Src& S, int v, int w, uint32_t& ra
     if (w > S.src) {
         if (v == S.src) {
             raw++;
-            if (fresh) orig++;
+            if (S.chained) orig += hset_insert(w);
+            else if (fresh) orig++;
         }
         return false;
     }
@@ -273,7 +309,7 @@ __device__ __forceinline__ void td_level(const Src& S, int32_t* q, long long qca
         int s0 = 0, plen = 0;
         if (i < le) {
             bool skip = false;
-            if (S.merged_mask) skip = v == S.src || covered(S, S.top, v);
+            if (S.merged_mask && i < S.qmark) skip = v == S.src || covered(S, S.top, v);
             if (!skip) {
                 const int r0 = ld_i32<CG>(S.rp + v), r1 = ld_i32<CG>(S.rp + v + 1);
                 s0 = r0 & ~3;
@@ -650,7 +686,8 @@ __device__ __forceinline__ void flush_counters(unsigned long long* c, unsigned l
     atomicAdd(&c[CNT_EDGES_TRAV], acc[3]);
     atomicAdd(&c[CNT_NNZ_U], acc[4]);
     atomicAdd(&c[CNT_NNZ_L], acc[5]);
-    for (int j = 0; j < 6; j++) acc[j] = 0;
+    if (acc[6]) atomicAdd(&c[CNT_CHAINED], acc[6]);
+    for (int j = 0; j < 7; j++) acc[j] = 0;
 }
 
 // MODE 0: each CTA's bitmap in global memory; 1: in shared memory;
@@ -673,6 +710,7 @@ __global__ void __launch_bounds__(BLOCK, 1024 / BLOCK) traverse_kernel(TraverseL
     } else if (threadIdx.x == 0) {
         SM.cta = blockIdx.x;
     }
+    if (threadIdx.x == 0) SM.chain = 0;
     const long long cta = MODE == 2 ? SM.cta : blockIdx.x;
     uint32_t* const sbm = reinterpret_cast<uint32_t*>(dyn_smem);
     uint32_t* const gbm = MODE == 1 ? nullptr : P.gbitmap + cta * P.bitmap_words;
@@ -690,7 +728,7 @@ __global__ void __launch_bounds__(BLOCK, 1024 / BLOCK) traverse_kernel(TraverseL
     // thread 0 accumulates per-matrix counters and flushes on matrix change
     // (serving: after every item)
     int acc_mat = -1;
-    unsigned long long acc[6] = {0, 0, 0, 0, 0, 0};
+    unsigned long long acc[7] = {0, 0, 0, 0, 0, 0, 0};
     const long long stride = P.sample_stride > 1 ? P.sample_stride : 1;
 
     for (;;) {
@@ -773,6 +811,11 @@ __global__ void __launch_bounds__(BLOCK, 1024 / BLOCK) traverse_kernel(TraverseL
             S.top = -1;
             S.pending = 0ull;
             S.reached = &SM.reached[0];
+            S.qmark = 0;
+            // the bitmap still holds the closure of src - 1 (decided by its census)
+            S.chained = SM.chain != 0;
+            if (S.chained)
+                for (int i = threadIdx.x; i < kHsetCap; i += BLOCK) chain_hset[i] = -1;
             if (threadIdx.x == 0) {
                 bm[src >> 5] |= 1u << (src & 31);
                 q[0] = src;
@@ -780,7 +823,12 @@ __global__ void __launch_bounds__(BLOCK, 1024 / BLOCK) traverse_kernel(TraverseL
                 SM.grab[0] = 0;
                 SM.reached[0] = 0ull;
                 SM.abort_level = 0;
-                SM.wlo = SM.whi = src >> 5;
+                if (S.chained) {  // the census range covers the kept bits too
+                    SM.wlo = min(SM.wlo, src >> 5);
+                    SM.whi = max(SM.whi, src >> 5);
+                } else {
+                    SM.wlo = SM.whi = src >> 5;
+                }
             }
             __syncthreads();
             // this thread's share of the set bits' word range
@@ -826,6 +874,7 @@ __global__ void __launch_bounds__(BLOCK, 1024 / BLOCK) traverse_kernel(TraverseL
                         const int np = did ? SM.pushed : 0;
                         S.pending = did ? (SM.pending & ~mm) : (S.pending & ~mm);
                         le = le + nxt + np;  // redo this level (it may have been cut short)
+                        S.qmark = (int)le;   // later entries are outside the merged closures
                     } else {
                         lb = le;
                         le = le + nxt;
@@ -860,6 +909,7 @@ __global__ void __launch_bounds__(BLOCK, 1024 / BLOCK) traverse_kernel(TraverseL
                         __syncthreads();
                         S.pending = did ? (SM.pending & ~mm) : (S.pending & ~mm);
                         le = le + (did ? SM.pushed : 0);  // merged-in ids become queue entries
+                        S.qmark = (int)le;
                         continue;  // sweep again with the merged closure
                     }
                     if (found == 0) break;
@@ -879,8 +929,29 @@ __global__ void __launch_bounds__(BLOCK, 1024 / BLOCK) traverse_kernel(TraverseL
                 atomicMin(&SM.wlo, wl);
                 atomicMax(&SM.whi, wh);
             }
+            if (threadIdx.x == 0) {
+                // src + 1 in this closure: publish it for the other direction's
+                // search of src + 1, then decide whether src + 1 chains (the
+                // search is over: every bit is final after its last barrier)
+                const int32_t nx = src + 1;
+                const bool nbit = nx < n && ((ld_vol(bm + (nx >> 5)) >> (nx & 31)) & 1u);
+                if (M.link && !lfold && !P.pattern_pass)
+                    *reinterpret_cast<volatile uint8_t*>(M.link + 2ll * src + dir) = nbit ? 2 : 1;
+                int ch = 0;
+                if (P.chain && P.bu_alpha <= 0 && nx < s_end) {
+                    const int r0 = ld_i32<CG>(S.rp + nx), r1 = ld_i32<CG>(S.rp + nx + 1);
+                    if ((r1 & ~3) - (r0 & ~3) <= kChainMaxRow) {
+                        if (lfold) ch = nbit;  // symmetric: U(src, src+1) = L(src+1, src)
+                        else if (M.link)
+                            ch = *reinterpret_cast<const volatile uint8_t*>(
+                                     M.link + 2ll * src + (1 - dir)) == 2;
+                    }
+                }
+                SM.chain = ch;
+            }
             __syncthreads();
             const long long wlo = SM.wlo, whi = SM.whi;
+            const bool chain_next = SM.chain != 0;
 
             if ((dir == 1 || lfold) && !P.pattern_pass && threadIdx.x < 4) {
                 // 128-bit mask of rows f+1 .. f+128 in L column f (supernode test)
@@ -938,7 +1009,7 @@ __global__ void __launch_bounds__(BLOCK, 1024 / BLOCK) traverse_kernel(TraverseL
             // every set bit lies in words [wlo, whi]: the rest of the bitmap is zero
             for (long long w = wlo + threadIdx.x; w <= whi; w += BLOCK) {
                 const uint32_t x = bm[w];
-                bm[w] = 0u;
+                if (!chain_next) bm[w] = 0u;
                 if (keep) keep_slot[w] = x;
                 if (!x || w >= nwords) continue;
                 const long long base = w << 5;
@@ -1030,6 +1101,7 @@ __global__ void __launch_bounds__(BLOCK, 1024 / BLOCK) traverse_kernel(TraverseL
                     acc[4] += gt;
                 }
                 if (dir == 1 || lfold) acc[5] += gt;
+                acc[6] += S.chained ? 1 : 0;
             }
             __syncthreads();
         }

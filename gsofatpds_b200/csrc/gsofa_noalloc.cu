@@ -13,36 +13,32 @@
 // The array is a file-scope __device__ object: every GPU that loads this
 // library holds GSOFA_NOALLOC_SCRATCH_BYTES for it until the process exits.
 // Host code cannot use the symbol itself as a device address (on the host it
-// names a stand-in); the address is taken with cudaGetSymbolAddress once per
-// device, with that device current, on the first call made for that device.
+// names a stand-in); every call looks the address up with
+// cudaGetSymbolAddress, with the matrix's device current, so no address is
+// kept across calls (a context reset between calls leaves nothing stale).
 // Calls share the array: the work counter and the status word are cleared
 // on every call, and two calls that overlap on the GPU race on it.
+//
+// Launch shape: the main entry point's defaults (gsofa_host.h) except the
+// closure ring, which defaults to kNoallocRing slots instead of kDefaultRing:
+// every CTA's queue and ring come out of the one fixed array, and a 64-deep
+// ring (8n bytes per CTA) would leave about a quarter of the CTAs that the
+// 8-deep one leaves at n ~ 600k.
 #include <cuda_runtime.h>
 
-#include <mutex>
-
 #include "../../include/gsofa.h"
+#include "gsofa_host.h"
 #include "gsofa_internal.h"
 
 namespace {
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[GSOFA_NOALLOC_SCRATCH_BYTES];
 
-constexpr int kMaxDevices = 64;
-std::mutex g_mu;
-void* g_scratch_ptr[kMaxDevices] = {};
+constexpr int kNoallocRing = 8;
 
-// Device address of the scratch array on `device` (the current device).
-cudaError_t scratch_address(int device, void** out) {
-    std::lock_guard<std::mutex> g(g_mu);
-    if (!g_scratch_ptr[device]) {
-        void* p = nullptr;
-        cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-        if (e != cudaSuccess) return e;
-        g_scratch_ptr[device] = p;
-    }
-    *out = g_scratch_ptr[device];
-    return cudaSuccess;
+// Device address of the scratch array on the current device.
+cudaError_t scratch_address(void** out) {
+    return cudaGetSymbolAddress(out, g_noalloc_scratch);
 }
 
 size_t round256(size_t x) { return (x + 255) & ~(size_t)255; }
@@ -70,7 +66,6 @@ extern "C" int gsofa_factor_symbolic_noalloc(const gsofa_matrix* mat, const gsof
     MatrixView mv;
     if (!matrix_view(mat, &mv)) return GSOFA_ERR_ARG;
     if (!d_nnz_u_row || !d_nz_row_u || !d_nnz_l_col || !d_lmask || !d_counters) return GSOFA_ERR_ARG;
-    if (mv.device < 0 || mv.device >= kMaxDevices) return GSOFA_ERR_UNSUPPORTED;
     gsofa_opts o;
     if (opts) {
         o = *opts;
@@ -88,7 +83,7 @@ extern "C" int gsofa_factor_symbolic_noalloc(const gsofa_matrix* mat, const gsof
     DeviceGuard guard(mv.device);
     cudaStream_t st = reinterpret_cast<cudaStream_t>(cuda_stream);
     void* base = nullptr;
-    if (scratch_address(mv.device, &base) != cudaSuccess) return GSOFA_ERR_CUDA;
+    if (scratch_address(&base) != cudaSuccess) return GSOFA_ERR_CUDA;
 
     const int32_t n = mv.n;
     const long long words = (((long long)n + 31) >> 5) + 6;
@@ -109,10 +104,9 @@ extern "C" int gsofa_factor_symbolic_noalloc(const gsofa_matrix* mat, const gsof
     if (occ <= 0) return GSOFA_ERR_UNSUPPORTED;
 
     const bool merge = !(o.flags & GSOFA_NO_MERGE);
-    int ring = o.cached_closures > 0 ? o.cached_closures : 8;
-    if (ring > 64) ring = 64;  // the kernel's ring masks hold 64 slots
+    int ring = o.cached_closures > 0 ? o.cached_closures : kNoallocRing;
+    if (ring > host::kMaxRing) ring = host::kMaxRing;
     while (ring & (ring - 1)) ring &= ring - 1;
-    const long long chunk = o.chunk_sources > 0 ? o.chunk_sources : 64;
 
     // scratch layout: [counter+status 256 B][descriptor][per-CTA queues]
     // [per-CTA closure rings][per-CTA global bitmaps when shared memory is too small]
@@ -125,6 +119,8 @@ extern "C" int gsofa_factor_symbolic_noalloc(const gsofa_matrix* mat, const gsof
     const long long fit = (long long)(((size_t)GSOFA_NOALLOC_SCRATCH_BYTES - head) / per_cta);
     if (grid > fit) grid = fit;
     if (o.sources_in_flight > 0 && grid > o.sources_in_flight) grid = o.sources_in_flight;
+    const long long chunk = o.chunk_sources > 0 ? o.chunk_sources
+                                                : host::default_chunk(2ll * n, (int)grid);
 
     unsigned char* b = static_cast<unsigned char*>(base);
     unsigned long long* work_counter = reinterpret_cast<unsigned long long*>(b);
@@ -169,17 +165,21 @@ extern "C" int gsofa_factor_symbolic_noalloc(const gsofa_matrix* mat, const gsof
     L.work_counter = work_counter;
     L.queue = queue;
     L.queue_stride = (long long)(round256((size_t)(n > 0 ? n : 1) * 4) / 4);
+    if (o.flags & GSOFA_DEBUG_QUEUE_CAP) L.queue_stride = L.queue_stride < 64 ? L.queue_stride : 64;
     L.gbitmap = gbm;
     L.bitmap_words = words;
     L.status = status;
     L.pattern_pass = 0;
-    L.bu_alpha = o.bu_alpha > 0 ? o.bu_alpha : 0;
-    L.bu_beta = o.bu_beta > 0 ? o.bu_beta : 24;
-    L.bu_min_src = o.bu_min_source > 0 ? o.bu_min_source : 2048;
-    L.heavy_len = o.heavy_row > 0 ? ((o.heavy_row + 3) & ~3) : 64;
+    L.bu_alpha = o.bu_alpha > 0 ? o.bu_alpha : (o.bu_alpha < 0 ? 0 : host::kDefaultBuAlpha);
+    L.bu_beta = o.bu_beta > 0 ? o.bu_beta : host::kDefaultBuBeta;
+    L.bu_min_src = o.bu_min_source > 0 ? o.bu_min_source : host::kBuMinSource;
+    L.heavy_len = o.heavy_row > 0 ? ((o.heavy_row + 3) & ~3) : host::kDefaultHeavyRow;
     L.gprev = rings;
     L.chunk = (int)chunk;
     L.merge = merge ? 1 : 0;
+    // chained starts of symmetric patterns only: the links between the two
+    // directions of unsymmetric ones would need result storage (d.link stays null)
+    L.chain = merge && !(o.flags & GSOFA_NO_CHAIN) ? 1 : 0;
     L.ring = ring;
     if (L.total_items > 0) {
         e = launch_traverse(L, block, (int)grid, smem_bitmap, smem_bitmap ? bm_bytes : 0, st);
@@ -194,7 +194,5 @@ extern "C" int gsofa_factor_symbolic_noalloc(const gsofa_matrix* mat, const gsof
     e = cudaMemcpyAsync(&h_status, status, sizeof(h_status), cudaMemcpyDeviceToHost, st);
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);
     if (e != cudaSuccess) return GSOFA_ERR_CUDA;
-    if (h_status & DEV_ERR_QUEUE) return GSOFA_ERR_OVERFLOW;
-    if (h_status) return GSOFA_ERR_ARG;
-    return GSOFA_OK;
+    return device_status_code(h_status);
 }

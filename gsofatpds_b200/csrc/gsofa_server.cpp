@@ -361,6 +361,7 @@ bool launch_kernel(gsofa_server* s, int k, int grid) {
     L.gprev = s->rings;
     L.chunk = 1;
     L.merge = s->merge ? 1 : 0;
+    L.chain = s->merge && !(s->opts.flags & GSOFA_NO_CHAIN) ? 1 : 0;
     L.ring = s->ring;
     L.sample_stride = 1;
     L.bitmap_words = s->words;
@@ -504,6 +505,7 @@ bool reap(gsofa_server* s) {
             k.edges_alg = c[CNT_EDGES_ALG];
             k.vertices_alg = c[CNT_VERTS_ALG];
             k.edges_traversed = c[CNT_EDGES_TRAV];
+            k.sources_chained = c[CNT_CHAINED];
             const double t = now_ms(s);
             k.ms_device = t - r->t_publish;  // host clock: publication to completion
             k.ms_traverse = k.ms_device;

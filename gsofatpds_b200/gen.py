@@ -218,12 +218,16 @@ def batch_mix(count=512, nmin=2000, nmax=60000, seed=4):
     return mats
 
 
-def request_stream(count=64, rate_hz=20.0, nmin=1000, nmax=1000000, seed=5, max_rb_n=None):
+def request_stream(count=64, rate_hz=20.0, nmin=1000, nmax=1000000, seed=5, max_rb_n=None,
+                   big_n=None):
     """Serving stream: Poisson arrivals at `rate_hz`; each request is a seeded
     matrix with n log-uniform in [nmin, nmax] and 5-27 nnz/row: 2D 5/9-point
     and 3D 7/27-point grid patterns in nested-dissection order, or
-    random-banded unsymmetric.  Returns [(arrival_s, kind, spec)] where spec
-    is passed to ``make_request``."""
+    random-banded unsymmetric.  Random-banded requests are capped at
+    `max_rb_n` rows (their fill grows as n^2).  A draw of at least `big_n`
+    rows becomes the stream's largest request kind, the 3D 27-point grid of
+    side round(nmax^(1/3)) (100^3: n = 1,000,000, ~26.5M nnz).  Returns
+    [(arrival_s, kind, spec)] where spec is passed to ``make_request``."""
     rng = np.random.default_rng(seed)
     t = 0.0
     out = []
@@ -234,8 +238,18 @@ def request_stream(count=64, rate_hz=20.0, nmin=1000, nmax=1000000, seed=5, max_
         kind = kinds[int(rng.integers(0, len(kinds)))]
         if kind == "banded" and max_rb_n is not None:
             n_t = min(n_t, max_rb_n)
+        if big_n is not None and n_t >= big_n:
+            kind = "grid3d_27"
+            n_t = int(round(nmax ** (1.0 / 3.0))) ** 3
         out.append((t, kind, dict(n=n_t, seed=int(rng.integers(1 << 30)))))
     return out
+
+
+# the serving benchmark's stream: 48 requests at 20/s, random-banded
+# requests capped at 100,000 rows, draws of 500,000 rows or more become
+# 100^3 27-point grids
+SERVE_STREAM = dict(count=48, rate_hz=20.0, nmin=1000, nmax=1000000, seed=5, max_rb_n=100000,
+                    big_n=500000)
 
 
 def make_request(kind, spec):

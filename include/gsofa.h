@@ -54,8 +54,12 @@ typedef struct gsofa_batch gsofa_batch;
 /* Fault injection: each CTA's frontier queue holds only 64 entries, so any
  * search that queues more reports GSOFA_ERR_OVERFLOW (every queue access is
  * bounds-checked; nothing is written past the bound).  gsofa_factor_symbolic
- * only. */
+ * and gsofa_factor_symbolic_noalloc. */
 #define GSOFA_DEBUG_QUEUE_CAP (1u << 28)
+/* Diagnostic: never start a source's search from the previous source's
+ * closure (the start the traversal takes when the other direction's search
+ * has shown that the previous source is reachable); merges stay on. */
+#define GSOFA_NO_CHAIN (1u << 27)
 
 typedef struct gsofa_opts {
     /* rows per supernode chunk; the reference's max_supernode_size, argv[5]
@@ -224,6 +228,8 @@ typedef struct gsofa_counts {
     uint64_t edges_traversed; /* edge inspections this engine made (A and A^T)  */
     double ms_device;         /* device time of the factorization (CUDA events) */
     double ms_traverse;       /* device time of the traversal kernel alone      */
+    uint64_t sources_chained; /* source searches (U rows and L columns) that
+                               * started from the previous source's closure    */
 } gsofa_counts;
 int gsofa_result_counts(const gsofa_result* res, gsofa_counts* out);
 
@@ -353,10 +359,11 @@ const char* gsofa_server_last_error(const gsofa_server* srv);
  *     cached_closures * (n/8 + 24) bytes of closure ring per CTA (plus n/8
  *     bytes of bitmap when n > ~1.8M); the grid shrinks to what fits and
  *     GSOFA_ERR_SCRATCH is returned when not even one CTA fits (n above
- *     roughly 12M with the default 8 cached closures).
- *   - The first call made for a device looks up the array's device address
- *     (cudaGetSymbolAddress) with that device current; make that first call
- *     before any stream capture.
+ *     roughly 12M with the default 8 cached closures).  Other launch
+ *     defaults are those of gsofa_factor_symbolic; the ring defaults to 8
+ *     slots (not 64) so that more CTAs fit the fixed array.
+ *   - Every call looks up the array's device address (cudaGetSymbolAddress)
+ *     with the matrix's device current; no address is kept between calls.
  *   - Every call shares the array and leaves its contents behind; the work
  *     counter and status word are cleared by each call.  Calls that overlap
  *     on the GPU (other streams, other threads) race on the array.
@@ -365,9 +372,12 @@ const char* gsofa_server_last_error(const gsofa_server* srv);
  *     as gsofa_result_lmask; d_supernode_flags n bytes (needed only with
  *     GSOFA_SUPERNODES); d_counters 8 entries: fills, edges_alg,
  *     vertices_alg, edges_traversed, supernodes detected (printed count - 1),
- *     nnz_u, nnz_l, unused.
+ *     nnz_u, nnz_l, sources chained.
  *   - GSOFA_L_ROW_STATS and GSOFA_PATTERN are not available here; digests are
- *     not computed.  Synchronous on cuda_stream (NULL = legacy stream). */
+ *     not computed.  Errors map as in gsofa_factor_symbolic (a queue bound
+ *     exceeded, e.g. under GSOFA_DEBUG_QUEUE_CAP: GSOFA_ERR_OVERFLOW).
+ *   - Synchronous: returns after the work queued on cuda_stream (NULL =
+ *     legacy stream) has finished. */
 #define GSOFA_NOALLOC_SCRATCH_BYTES (64u << 20)
 int gsofa_factor_symbolic_noalloc(const gsofa_matrix* mat, const gsofa_opts* opts,
                                   void* cuda_stream, int32_t* d_nnz_u_row, int32_t* d_nz_row_u,

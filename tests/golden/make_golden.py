@@ -10,7 +10,7 @@ reference tree; the fixtures themselves travel without it).
                  space_optimization_log_1_264_GPU_warp_centric.dat:2) and the
                  oracle's derived totals
 
-Usage: python tests/golden/make_golden.py [/path/to/reference]
+Usage: python tests/golden/make_golden.py /path/to/gSoFaTPDS
 """
 import json
 import os
@@ -27,7 +27,9 @@ PUBLISHED_BC_FILLS = 980136
 
 
 def main():
-    ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    if len(sys.argv) != 2:
+        raise SystemExit("usage: make_golden.py /path/to/gSoFaTPDS (the reference checkout)")
+    ref = sys.argv[1]
     d = os.path.join(ref, "SpaceOptimization", "dataset")
     beg, end, col = O.read_dat(os.path.join(d, "colbeg_11948.dat"),
                                os.path.join(d, "colend_11948.dat"),
