@@ -72,23 +72,31 @@ def read_peaks():
     return 6650.0, "fallback"
 
 
-def roofline_entry(edges, vertices_alg, n, kernel_ms, peak, peak_kind, traffic):
-    """The line's roofline object for the traversal kernel.  `achieved` is
-    the algorithmic bytes (8 E_alg + 16 V_alg + 4 W_out) per second of the
-    kernel; closure reuse makes it exceed the HBM peak.  `traffic` is the
-    DRAM bytes one launch really moves (ncu), and traffic_achieved /
-    traffic_frac are that rate against the same peak."""
+def roofline_entry(edges, vertices_alg, edges_trav, n, kernel_ms, peak, peak_kind, traffic):
+    """The line's roofline object for the traversal kernel, whose bound is
+    HBM (an irregular integer traversal; no tensor cores).  `achieved` is the
+    DRAM bytes one launch really moves (`traffic`: ncu dram__bytes_read.sum +
+    dram__bytes_write.sum of one full-size launch, from the committed
+    profile of this workload) per second of the kernel's CUDA-event time, and
+    frac = achieved / the measured HBM peak.  `work_equivalent` gives the
+    algorithmic bytes 8 E_alg + 16 V_alg + 4 W_out of a search that expands
+    every reachable vertex of every source, per second: closure reuse and
+    chained starts do far less than that work, so that figure exceeds the
+    peak and is not a bandwidth fraction."""
     w_out = 11 * n  # nnz_u, nz_row_u, nnz_lc, 2 digests (u64), 128-bit L-mask per row
     bytes_alg = 8 * edges + 16 * vertices_alg + 4 * w_out
-    achieved = bytes_alg / (kernel_ms / 1e3) / 1e9
-    roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-            "frac": achieved / peak, "traffic": traffic,
-            "peak_kind": peak_kind + " (MEASURED_PEAKS hbm_gbs)",
+    t = kernel_ms / 1e3
+    roof = {"bound": "hbm", "achieved": None, "peak": peak, "unit": "GB/s", "frac": None,
+            "traffic": traffic, "peak_kind": peak_kind + " (MEASURED_PEAKS hbm_gbs)",
             "kernel": "traverse_kernel", "kernel_ms": kernel_ms,
-            "bytes_alg": bytes_alg}
+            "traffic_source": "ncu, one full-size launch (profiles/traverse_<workload>.md)",
+            "inspected_edges_per_s": edges_trav / t,
+            "work_equivalent": {"bytes_alg": bytes_alg, "gbs": bytes_alg / t / 1e9,
+                                "note": "algorithmic bytes of an ideal label search per second; "
+                                        "the kernel reuses closures, so this exceeds the peak"}}
     if traffic:
-        roof["traffic_achieved"] = traffic / (kernel_ms / 1e3) / 1e9
-        roof["traffic_frac"] = roof["traffic_achieved"] / peak
+        roof["achieved"] = traffic / t / 1e9
+        roof["frac"] = roof["achieved"] / peak
     return roof
 
 
@@ -220,20 +228,17 @@ def run_reference(args, rank, world):
     print(json.dumps(line), flush=True)
 
 
-def run_batch(args, local):
-    """Batched form: the same 512 matrices factored back to back (one call
-    each) and as one graph-captured persistent launch."""
+def measure_batch(ctx, stream, steps, warmup, tune=True):
+    """Config 4: the 512-matrix mix factored as one graph-captured persistent
+    launch, against the same matrices factored back to back by plain calls
+    (each with its own autotuned shape, and with library defaults).  Device
+    time of each arm with CUDA events on `stream`, median over `steps`."""
     import torch
-    from gsofatpds_b200 import Context, gen
-    torch.cuda.set_device(local)
+    from gsofatpds_b200 import gen
     mats_np = gen.batch_mix(512)
-    ctx = Context(local)
-    stream = torch.cuda.Stream()
-    torch.cuda.set_stream(stream)
-    ctx.set_stream(stream.cuda_stream)
     mats = [ctx.load_rowptr(rp, col) for (_, rp, col) in mats_np]
     kw = dict(max_supernode_size=128)
-    if not args.no_tune:
+    if tune:
         kw.update(ctx.autotune_batch(mats, **kw))
     batch = ctx.batch(mats, **kw)
 
@@ -249,8 +254,7 @@ def run_batch(args, local):
     # plain arm: one call per matrix, each with its own tuned shape (the
     # tuner caches per size class), or the library defaults without tuning
     base = dict(max_supernode_size=128)
-    plain_kw = [dict(base, **ctx.autotune(m, **base)) for m in mats] if not args.no_tune \
-        else [base] * len(mats)
+    plain_kw = [dict(base, **ctx.autotune(m, **base)) for m in mats] if tune else [base] * len(mats)
 
     def plain():
         for m, k in zip(mats, plain_kw):
@@ -260,31 +264,47 @@ def run_batch(args, local):
         for m in mats:
             ctx.factor(m, **base).close()
 
-    for _ in range(args.warmup):
+    for _ in range(warmup):
         plain()
         plain_defaults()
         batch.run()
-    plain_ms = [timed(plain) for _ in range(args.steps)]
-    plain_def_ms = [timed(plain_defaults) for _ in range(args.steps)]
-    batch_ms = [timed(batch.run) for _ in range(args.steps)]
+    plain_ms = [timed(plain) for _ in range(steps)]
+    plain_def_ms = [timed(plain_defaults) for _ in range(steps)]
+    batch_ms = [timed(batch.run) for _ in range(steps)]
     edges = sum(batch.result(i).counts["edges_alg"] for i in range(len(mats)))
     pm, bm = float(np.median(plain_ms)), float(np.median(batch_ms))
-    line = {"metric": "matrices_per_s", "value": len(mats) / (bm / 1e3), "unit": "matrices/s",
-            "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": bm,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int32",
-            "data": "synthetic", "config": {"workload": WORKLOADS["batch512"],
-                                            "launch": {k: v for k, v in kw.items()}},
-            "plain_ms_per_batch": pm, "plain_matrices_per_s": len(mats) / (pm / 1e3),
-            "plain_shapes": "per-matrix autotuned" if not args.no_tune else "library defaults",
-            "speedup_vs_plain": pm / bm,
-            "plain_defaults_ms_per_batch": float(np.median(plain_def_ms)),
-            "speedup_vs_plain_defaults": float(np.median(plain_def_ms)) / bm,
-            "edges_alg": edges, "gteps": edges / (bm / 1e3) / 1e9,
-            "gpu_launches": 1}
-    print(json.dumps(line), flush=True)
+    pdm = float(np.median(plain_def_ms))
+    out = {"workload": WORKLOADS["batch512"], "matrices": len(mats),
+           "launch": {k: v for k, v in kw.items()},
+           "ms_per_batch": bm, "matrices_per_s": len(mats) / (bm / 1e3),
+           "plain_ms_per_batch": pm, "plain_matrices_per_s": len(mats) / (pm / 1e3),
+           "plain_shapes": "per-matrix autotuned" if tune else "library defaults",
+           "speedup_vs_plain": pm / bm,
+           "plain_defaults_ms_per_batch": pdm, "speedup_vs_plain_defaults": pdm / bm,
+           "edges_alg": edges, "gteps": edges / (bm / 1e3) / 1e9}
     batch.close()
     for m in mats:
         m.close()
+    return out
+
+
+def run_batch(args, local):
+    """Batched form on its own line (see measure_batch)."""
+    import torch
+    from gsofatpds_b200 import Context
+    torch.cuda.set_device(local)
+    ctx = Context(local)
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
+    ctx.set_stream(stream.cuda_stream)
+    r = measure_batch(ctx, stream, args.steps, args.warmup, tune=not args.no_tune)
+    line = {"metric": "matrices_per_s", "value": r["matrices_per_s"], "unit": "matrices/s",
+            "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": r["ms_per_batch"],
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int32",
+            "data": "synthetic", "config": {"workload": r["workload"], "launch": r["launch"]},
+            "gpu_launches": 1}
+    line.update({k: v for k, v in r.items() if k not in ("workload", "launch")})
+    print(json.dumps(line), flush=True)
     ctx.close()
 
 
@@ -535,22 +555,23 @@ def _pct(xs, q):
     return float(np.percentile(np.asarray(xs, dtype=np.float64), q)) if len(xs) else None
 
 
-def run_serve(args, local):
-    """Serving form: a seeded Poisson request stream replayed in real time
-    through the request loop (host CSR in, result counts out), against the
-    same requests served one at a time by plain calls (load + factor each,
-    back to back; their queueing under the same arrivals is replayed from the
-    measured service times)."""
-    import torch
-    from gsofatpds_b200 import Context, gen
-    torch.cuda.set_device(local)
-    spec = gen.request_stream(count=args.serve_count, rate_hz=args.serve_rate, nmin=1000,
-                              nmax=1000000, seed=5, max_rb_n=args.serve_max_banded)
-    reqs = [(t, kind, sp, gen.make_request(kind, sp)) for (t, kind, sp) in spec]
-    nmax = max(r[3][0] for r in reqs)
+def measure_serve(ctx, local, warmup, rate_hz, count, sampler=None):
+    """Config 5: the seeded request stream (gen.SERVE_STREAM: n log-uniform in
+    [1e3, 1e6], the largest requests 100^3 27-point grids) through the
+    request loop, against plain calls (load + factor, one at a time), both
+    measured on the host clock with host CSR in and results out:
+      saturated  every request submitted at once: makespan, matrices/s and
+                 latency from the common start, served vs plain back to back;
+      at_rate    Poisson arrivals at rate_hz replayed in real time: each arm
+                 measured as it runs (the plain arm starts a request when it
+                 has arrived and the previous one is done)."""
+    from gsofatpds_b200 import gen
+    cfg = dict(gen.SERVE_STREAM, count=count, rate_hz=rate_hz)
+    spec = gen.request_stream(**cfg)
+    reqs = [(t, gen.make_request(kind, sp)) for (t, kind, sp) in spec]
+    nmax = max(r[1][0] for r in reqs)
     kw = dict(max_supernode_size=128)
-    ctx = Context(local)
-    warm = [r for r in reqs if r[3][0] < 20000][:max(args.warmup, 1)]
+    warm = [r for r in reqs if r[1][0] < 20000][:max(warmup, 1)]
 
     def plain_one(rp, col):
         m = ctx.load_rowptr(rp, col)
@@ -560,74 +581,100 @@ def run_serve(args, local):
         m.close()
         return c
 
-    for r in warm:
-        plain_one(r[3][1], r[3][2])
-    service, plain_counts = [], []
-    for r in reqs:
-        t0 = time.perf_counter()
-        plain_counts.append(plain_one(r[3][1], r[3][2]))
-        service.append(time.perf_counter() - t0)
-    done, plain_lat = 0.0, []
-    for (t_arr, _, _, _), sv in zip(reqs, service):
-        done = max(done, t_arr) + sv
-        plain_lat.append(done - t_arr)
-    plain_makespan = done - reqs[0][0]
+    def plain_arm(arrivals):
+        start = time.perf_counter()
+        lat, counts, done = [], [], 0.0
+        for t_arr, (_, rp, col) in zip(arrivals, [r[1] for r in reqs]):
+            d = start + t_arr - time.perf_counter()
+            if d > 0:
+                time.sleep(d)
+            counts.append(plain_one(rp, col))
+            done = time.perf_counter() - start
+            lat.append(done - t_arr)
+        return lat, done - min(arrivals), counts
 
-    skw = dict(kw)
-    if args.threads_per_source:
-        skw["threads_per_source"] = args.threads_per_source
-    srv = ctx.server(max_n=nmax, budget_bytes=40 << 30, **skw)
+    def served_arm(srv, arrivals):
+        start = time.perf_counter()
+        tickets = []
+        for t_arr, (_, rp, col) in zip(arrivals, [r[1] for r in reqs]):
+            d = start + t_arr - time.perf_counter()
+            if d > 0:
+                time.sleep(d)
+            tickets.append(srv.submit_rowptr(rp, col))
+        counts = []
+        for t in tickets:
+            r = srv.wait(t)
+            counts.append(r.counts)
+            r.close()
+        info = [srv.info(t) for t in tickets]
+        t0 = min(i["t_submit_ms"] for i in info) - 1e3 * arrivals[0]
+        lat = [(i["t_done_ms"] - (t0 + 1e3 * a)) / 1e3 for i, a in zip(info, arrivals)]
+        makespan = (max(i["t_done_ms"] for i in info) - min(i["t_submit_ms"] for i in info)) / 1e3
+        return lat, makespan, counts, info
+
     for r in warm:
-        srv.wait(srv.submit_rowptr(r[3][1], r[3][2])).close()
-    sampler = ClockSampler(local)
-    sampler.start()
-    start = time.perf_counter()
-    tickets = []
-    for (t_arr, _, _, (_, rp, col)) in reqs:
-        d = start + t_arr - time.perf_counter()
-        if d > 0:
-            time.sleep(d)
-        tickets.append(srv.submit_rowptr(rp, col))
-    counts = []
-    for t in tickets:
-        r = srv.wait(t)
-        counts.append(r.counts)
-        r.close()
-    clk = sampler.stop()
-    info = [srv.info(t) for t in tickets]
+        plain_one(r[1][1], r[1][2])
+    k = len(reqs)
+    zero = [0.0] * k
+    arr = [r[0] for r in reqs]
+    p_lat0, p_span0, p_counts = plain_arm(zero)
+    p_lat1, p_span1, _ = plain_arm(arr)
+    srv = ctx.server(max_n=nmax, budget_bytes=40 << 30, **kw)
+    for r in warm:
+        srv.wait(srv.submit_rowptr(r[1][1], r[1][2])).close()
+    if sampler:
+        sampler.start()
+    s_lat0, s_span0, s_counts, _ = served_arm(srv, zero)
+    s_lat1, s_span1, _, info1 = served_arm(srv, arr)
+    clk = sampler.stop() if sampler else None
     st = srv.stats()
     srv.close()
-    ctx.close()
-    lat = [(i["t_done_ms"] - i["t_submit_ms"]) / 1e3 for i in info]
-    wait_admit = [(i["t_admit_ms"] - i["t_submit_ms"]) for i in info]
-    build = [(i["t_publish_ms"] - i["t_admit_ms"]) for i in info]
-    run = [(i["t_done_ms"] - i["t_publish_ms"]) for i in info]
-    makespan = (max(i["t_done_ms"] for i in info) - min(i["t_submit_ms"] for i in info)) / 1e3
     same = all(a["fill_count"] == b["fill_count"] and a["n_supernodes"] == b["n_supernodes"]
-               and a["edges_alg"] == b["edges_alg"] for a, b in zip(counts, plain_counts))
-    edges = sum(c["edges_alg"] for c in counts)
-    k = len(reqs)
-    h2d = sum(4 * (r[3][0] * 2 + r[3][2].shape[0]) for r in reqs)
-    line = {"metric": "matrices_per_s", "value": k / makespan, "unit": "matrices/s", "n_gpus": 1,
-            "steps": 1, "warmup": len(warm), "ms_per_step": makespan * 1e3,
+               and a["edges_alg"] == b["edges_alg"] for a, b in zip(s_counts, p_counts))
+    edges = sum(c["edges_alg"] for c in s_counts)
+    h2d = sum(4 * (r[1][0] * 2 + r[1][2].shape[0]) for r in reqs)
+    ms = lambda x, q: _pct(x, q) * 1e3  # noqa: E731
+    out = {"workload": WORKLOADS["serve"], "requests": k, "max_n": nmax,
+           "largest": "100^3 27-point grid (n=1,000,000)" if nmax >= 1000000 else None,
+           "banded_n_cap": cfg["max_rb_n"], "budget_gb": 40, "grid": st["grid"], "block": st["block"],
+           "identical_to_plain": same, "edges_alg": edges,
+           "saturated": {"matrices_per_s": k / s_span0, "plain_matrices_per_s": k / p_span0,
+                         "speedup_vs_plain": p_span0 / s_span0, "makespan_s": s_span0,
+                         "plain_makespan_s": p_span0, "p50_ms": ms(s_lat0, 50),
+                         "p99_ms": ms(s_lat0, 99), "plain_p50_ms": ms(p_lat0, 50),
+                         "plain_p99_ms": ms(p_lat0, 99), "gteps": edges / s_span0 / 1e9},
+           "at_rate": {"rate_hz": rate_hz, "matrices_per_s": k / s_span1,
+                       "plain_matrices_per_s": k / p_span1, "p50_ms": ms(s_lat1, 50),
+                       "p99_ms": ms(s_lat1, 99), "plain_p50_ms": ms(p_lat1, 50),
+                       "plain_p99_ms": ms(p_lat1, 99),
+                       "run_p50_ms": _pct([i["t_done_ms"] - i["t_publish_ms"] for i in info1], 50)},
+           "latency": "host clock from each request's arrival to its result; the plain arm "
+                      "measured in real time, not replayed",
+           "max_in_flight": st["max_in_flight"], "kernel_launches": st["kernel_launches"],
+           "peak_bytes": st["peak_bytes"], "h2d_bytes": h2d}
+    if clk:
+        out["clocks"] = clk
+    return out
+
+
+def run_serve(args, local):
+    """Serving form on its own line (see measure_serve)."""
+    import torch
+    from gsofatpds_b200 import Context
+    torch.cuda.set_device(local)
+    with Context(local) as ctx:
+        r = measure_serve(ctx, local, args.warmup, args.serve_rate, args.serve_count,
+                          ClockSampler(local))
+    sat = r["saturated"]
+    line = {"metric": "matrices_per_s", "value": sat["matrices_per_s"], "unit": "matrices/s",
+            "n_gpus": 1, "steps": 1, "warmup": args.warmup, "ms_per_step": sat["makespan_s"] * 1e3,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int32",
-            "data": "synthetic",
-            "config": {"workload": WORKLOADS["serve"], "requests": k, "rate_hz": args.serve_rate,
-                       "banded_n_cap": args.serve_max_banded, "max_n": nmax,
-                       "budget_gb": 40, "grid": st["grid"], "block": st["block"]},
-            "p50_ms": _pct(lat, 50) * 1e3, "p99_ms": _pct(lat, 99) * 1e3,
-            "plain_matrices_per_s": k / plain_makespan, "plain_p50_ms": _pct(plain_lat, 50) * 1e3,
-            "plain_p99_ms": _pct(plain_lat, 99) * 1e3, "speedup_vs_plain": plain_makespan / makespan,
-            "plain_service_s": float(sum(service)), "identical_to_plain": same,
-            "edges_alg": edges, "gteps": edges / makespan / 1e9,
-            "stage_ms": {"admit_wait_p50": _pct(wait_admit, 50), "build_p50": _pct(build, 50),
-                         "build_p99": _pct(build, 99), "run_p50": _pct(run, 50),
-                         "run_p99": _pct(run, 99)},
-            "max_in_flight": st["max_in_flight"], "kernel_launches": st["kernel_launches"],
-            "peak_bytes": st["peak_bytes"],
-            "e2e": {"value": k / makespan, "unit": "matrices/s", "h2d_bytes_per_step": h2d,
-                    "d2h_bytes_per_step": 8 * 8 * k},
-            "clocks": clk, "gpu_launches": st["kernel_launches"]}
+            "data": "synthetic", "config": {"workload": r["workload"], "requests": r["requests"],
+                                            "rate_hz": args.serve_rate, "max_n": r["max_n"]},
+            "e2e": {"value": sat["matrices_per_s"], "unit": "matrices/s",
+                    "h2d_bytes_per_step": r["h2d_bytes"], "d2h_bytes_per_step": 8 * 8 * r["requests"]},
+            "clocks": r.get("clocks"), "gpu_launches": r["kernel_launches"]}
+    line.update({k: v for k, v in r.items() if k not in ("workload", "clocks")})
     print(json.dumps(line), flush=True)
 
 
@@ -641,10 +688,13 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--threads-per-source", type=int, default=0)
     ap.add_argument("--no-tune", action="store_true", help="skip the autotuner (library defaults)")
+    ap.add_argument("--launch", default="",
+                    help="explicit launch shape threads,chunk,ring,heavy_row (skips the autotuner)")
     ap.add_argument("--serve-count", type=int, default=48)
     ap.add_argument("--serve-rate", type=float, default=20.0, help="Poisson arrivals per second")
-    ap.add_argument("--serve-max-banded", type=int, default=100000,
-                    help="largest random-banded request (their fill grows as n^2)")
+    ap.add_argument("--no-mix", action="store_true",
+                    help="default workload: skip the batch (config 4) and serving (config 5) "
+                         "measurements embedded in the line")
     ap.add_argument("--order-factor-all", action="store_true",
                     help="order workload: also factor the circuit-like matrix in both orders")
     args = ap.parse_args()
@@ -699,7 +749,11 @@ def main():
     kw = dict(max_supernode_size=mss, threads_per_source=args.threads_per_source)
 
     m = ctx.load_rowptr(rp, col)
-    if not args.no_tune and args.threads_per_source == 0:
+    if args.launch:
+        tps, chunk, ring, heavy = (int(x) for x in args.launch.split(","))
+        kw.update(threads_per_source=tps, chunk_sources=chunk, cached_closures=ring,
+                  heavy_row=heavy)
+    elif not args.no_tune and args.threads_per_source == 0:
         # the library's autotuner picks the launch shape (untimed, cached)
         kw.update(ctx.autotune(m, max_supernode_size=mss))
     # L2 flush buffer (> 126 MB L2) written between timed steps
@@ -779,8 +833,8 @@ def main():
     if rank == 0:
         peak, peak_kind = read_peaks()
         trav = float(np.mean(trav_ms))
-        roof = roofline_entry(edges, counts["vertices_alg"], n, trav, peak, peak_kind,
-                              read_traffic(args.workload))
+        roof = roofline_entry(edges, counts["vertices_alg"], counts["edges_traversed"], n, trav,
+                              peak, peak_kind, read_traffic(args.workload))
         line = {"metric": "fill_path_gteps", "value": value, "unit": "GTEPS", "n_gpus": world,
                 "steps": args.steps, "warmup": args.warmup,
                 "ms_per_step": max_ms / args.steps, "higher_is_better": True,
@@ -792,6 +846,10 @@ def main():
                 "ms_per_matrix": max_ms / args.steps, "matrices_per_s": world * args.steps / (max_ms / 1e3),
                 "fill_count": counts["fill_count"], "nnz_lu": counts["nnz_lu"],
                 "n_supernodes": counts["n_supernodes"], "edges_alg": edges,
+                "value_kind": "work-equivalent GTEPS: edges_alg (the reference's traversed-edge "
+                              "count without re-expansions) per second of device time",
+                "inspected_gteps": counts["edges_traversed"] / (max_ms / args.steps / 1e3) / 1e9,
+                "sources_chained": counts["sources_chained"],
                 "roofline": roof,
                 "e2e": {"value": e2e_value, "unit": "GTEPS", "h2d_bytes_per_step": h2d,
                         "d2h_bytes_per_step": d2h, "ms_per_step": float(np.mean(e2e_ms))},
@@ -799,6 +857,13 @@ def main():
                 "gpu_launches": 2 * args.steps}
         if world == 1 and args.cpu_seconds > 0:
             line["cpu_baseline"] = cpu_sample(rp, col, args.cpu_seconds)
+        if world == 1 and args.workload == "circuit_like" and not args.no_mix:
+            # the batched (config 4) and served (config 5) forms against plain
+            # calls, measured in the same run
+            line["batch"] = measure_batch(ctx, stream, args.steps, args.warmup,
+                                          tune=not args.no_tune)
+            line["serve"] = measure_serve(ctx, local, args.warmup, args.serve_rate,
+                                          args.serve_count)
         print(json.dumps(line), flush=True)
 
     m.close()

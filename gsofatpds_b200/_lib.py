@@ -60,7 +60,8 @@ class Opts(ctypes.Structure):
                 ("bu_min_source", ctypes.c_int32),
                 ("chunk_sources", ctypes.c_int32),
                 ("cached_closures", ctypes.c_int32),
-                ("reserved", ctypes.c_int32 * 2)]
+                ("chain_wait_us", ctypes.c_int32),
+                ("reserved", ctypes.c_int32)]
 
 
 class Counts(ctypes.Structure):

@@ -100,11 +100,12 @@ class Context:
              supernodes=True, digests=True, l_row_stats=False, pattern=False,
              bu_alpha=0, bu_beta=0, heavy_row=0, bu_min_source=0, chunk_sources=0,
              merge=True, cached_closures=0, global_bitmap=False, debug_queue_cap=False,
-             chain=True):
+             chain=True, chain_wait_us=0):
         """A gsofa_opts from keyword arguments (0 = library default); the
         launch-shape options change speed only, never results."""
         o = C.Opts()
         o.cached_closures = int(cached_closures)
+        o.chain_wait_us = int(chain_wait_us)
         o.chunk_sources = int(chunk_sources)
         o.bu_min_source = int(bu_min_source)
         o.bu_alpha = int(bu_alpha)

@@ -96,14 +96,32 @@ size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
 
 long long bitmap_words(int32_t n) { return (((long long)n + 31) >> 5) + 6; }
 
-// Default chunk (consecutive sources per work item): about four chunks per
-// CTA so the dynamic schedule can balance, between 16 and 512 sources.  Long
-// chunks amortise each chunk's first source, which has nothing to reuse.
+// Default chunk (consecutive sources per work item): about one chunk per
+// CTA, a power of 2 between 16 and 512 sources.  Each chunk's first source
+// starts cold (nothing to reuse), while later ones mostly start from their
+// predecessor's closure, so long chunks pay; the autotuner tries shorter
+// ones for matrices whose costly sources cluster (nested-dissection orders
+// put them in the top separators).
 long long default_chunk(long long total_sources, int grid) {
-    long long c = total_sources / (4ll * (grid > 0 ? grid : 1));
+    long long c = total_sources / (grid > 0 ? grid : 1);
     long long p = 16;
     while (p * 2 <= c && p < 512) p *= 2;
     return p;
+}
+
+long long work_sources(gsofa_ctx* ctx, const gsofa_matrix* m) {
+    if (m->host_sym < 0) {
+        int sym = 0;
+        if (m->n > 0 &&
+            cudaMemcpyAsync(ctx->h_status + 1, m->asym, 4, cudaMemcpyDeviceToHost, ctx->stream) ==
+                cudaSuccess &&
+            cudaStreamSynchronize(ctx->stream) == cudaSuccess)
+            sym = ctx->h_status[1] == 0;
+        else
+            cudaGetLastError();
+        m->host_sym = sym;
+    }
+    return (m->host_sym ? 1ll : 2ll) * m->n;
 }
 
 // Default CTA size: about 1024 resident threads per SM (the kernel is held
@@ -298,7 +316,7 @@ int run_factor(gsofa_ctx* ctx, const gsofa_matrix* const* mats, int32_t count,
     long long total_sources = 0;
     for (int32_t i = 0; i < count; i++) {
         nmax = std::max(nmax, mats[i]->n);
-        total_sources += 2ll * mats[i]->n;
+        total_sources += work_sources(ctx, mats[i]);
     }
     LaunchCfg cfg;
     int rc = plan_launch(ctx, std::max(nmax, 1), o, &cfg);
@@ -356,6 +374,7 @@ int run_factor(gsofa_ctx* ctx, const gsofa_matrix* const* mats, int32_t count,
     L.gprev = reinterpret_cast<uint32_t*>(ctx->gprev);
     L.merge = merge ? 1 : 0;
     L.chain = merge && !(o->flags & GSOFA_NO_CHAIN) ? 1 : 0;
+    L.chain_wait_ns = chain_wait_ns(*o);
     L.ring = ring;
     L.chunk = (int)chunk;
     L.heavy_len = o->heavy_row > 0 ? ((o->heavy_row + 3) & ~3) : kDefaultHeavyRow;
@@ -708,7 +727,8 @@ int gsofa_opts_default(gsofa_opts* o) {
     o->bu_min_source = 0;
     o->chunk_sources = 0;
     o->cached_closures = 0;
-    o->reserved[0] = o->reserved[1] = 0;
+    o->chain_wait_us = 0;
+    o->reserved = 0;
     return GSOFA_OK;
 }
 
@@ -903,11 +923,11 @@ static int autotune_impl(gsofa_ctx* ctx, const gsofa_matrix* const* mats, int32_
     int rc = GSOFA_OK;
     int32_t nmax = 0;
     long long total_sources = 0;
+    if (cudaSetDevice(ctx->device) != cudaSuccess) return set_err(ctx, GSOFA_ERR_CUDA, "cudaSetDevice");
     for (int32_t i = 0; i < count; i++) {
         nmax = std::max(nmax, mats[i]->n);
-        total_sources += 2ll * mats[i]->n;
+        total_sources += work_sources(ctx, mats[i]);
     }
-    if (cudaSetDevice(ctx->device) != cudaSuccess) return set_err(ctx, GSOFA_ERR_CUDA, "cudaSetDevice");
     gsofa_opts base = *opts;
     base.flags &= ~(uint32_t)(GSOFA_SUPERNODES | GSOFA_PATTERN | GSOFA_L_ROW_STATS);
     // reference timing with the defaults picks the sampling rate
@@ -986,7 +1006,7 @@ static int autotune_impl(gsofa_ctx* ctx, const gsofa_matrix* const* mats, int32_
         if (plan_launch(ctx, nmax, &best, &c) == GSOFA_OK) auto_chunk = default_chunk(total_sources, c.grid);
         ctx->err.clear();
         if (best.chunk_sources <= 0) best.chunk_sources = (int32_t)auto_chunk;
-        const long long cands[] = {auto_chunk / 4, auto_chunk * 2};
+        const long long cands[] = {auto_chunk / 8, auto_chunk / 4, auto_chunk / 2, auto_chunk * 2};
         for (long long ch : cands) {
             if (ch < 16 || ch > 1024 || ch == best.chunk_sources) continue;
             gsofa_opts p = best;
@@ -1113,9 +1133,9 @@ int gsofa_batch_create(gsofa_ctx* ctx, const gsofa_matrix* const* mats, int32_t 
         if (!mats[i] || mats[i]->ctx != ctx)
             return set_err(ctx, GSOFA_ERR_ARG, "matrix %d is null or from another context", i);
         nmax = std::max(nmax, mats[i]->n);
-        total_sources += 2ll * mats[i]->n;
     }
     if (cudaSetDevice(ctx->device) != cudaSuccess) return set_err(ctx, GSOFA_ERR_CUDA, "cudaSetDevice");
+    for (int32_t i = 0; i < count; i++) total_sources += work_sources(ctx, mats[i]);
     gsofa_batch* b = new (std::nothrow) gsofa_batch();
     if (!b) return set_err(ctx, GSOFA_ERR_OOM_BUDGET, "host allocation failed");
     b->ctx = ctx;
@@ -1207,6 +1227,7 @@ int gsofa_batch_create(gsofa_ctx* ctx, const gsofa_matrix* const* mats, int32_t 
     L.chunk = (int)chunk;
     L.merge = merge ? 1 : 0;
     L.chain = merge && !(o.flags & GSOFA_NO_CHAIN) ? 1 : 0;
+    L.chain_wait_ns = chain_wait_ns(o);
     L.ring = ring;
     L.sample_stride = 1;
 

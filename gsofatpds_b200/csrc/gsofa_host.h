@@ -57,6 +57,7 @@ struct gsofa_matrix {
     int32_t nplanes = 0;
     int32_t* asym = nullptr;  // device word: 0 iff the pattern is symmetric
     size_t bytes = 0;
+    mutable int host_sym = -1;  // the device word read back once (-1: not yet)
 };
 
 struct gsofa_result {
@@ -131,6 +132,10 @@ int dev_alloc_on(gsofa_ctx* ctx, size_t bytes, void** p, cudaStream_t stream);
 void dev_free_on(gsofa_ctx* ctx, void* p, size_t bytes, cudaStream_t stream);
 size_t align256(size_t x);
 long long default_chunk(long long total_sources, int grid);
+// Source searches a factorization of m runs: n for a symmetric pattern (the
+// U-row searches fill both halves), else 2n.  Reads the ingest's symmetry
+// word back once (synchronous on ctx->stream) and keeps it with m.
+long long work_sources(gsofa_ctx* ctx, const gsofa_matrix* m);
 int default_block(int32_t nmax, int smem_per_sm);
 // Result arrays of an n-row matrix, zero-initialised on `stream`.
 int result_alloc_on(gsofa_ctx* ctx, int32_t n, uint32_t flags, int32_t mss, cudaStream_t stream,
@@ -186,6 +191,13 @@ constexpr int kBuMinSource = 2048;
 constexpr int kDefaultHeavyRow = 16;  // padded rows above it are walked by a whole warp
 constexpr int kDefaultRing = 64;
 constexpr int kMaxRing = 64;  // the kernel's ring masks hold 64 slots
+// a source search waits up to this long for the other direction's result
+// when that search is one source behind (chained starts)
+constexpr int kDefaultChainWaitUs = 300;
+inline long long chain_wait_ns(const gsofa_opts& o) {
+    const int us = o.chain_wait_us > 0 ? o.chain_wait_us : (o.chain_wait_us < 0 ? 0 : kDefaultChainWaitUs);
+    return 1000ll * us;
+}
 // rows longer than this skip the ingest's symmetry check (its cost grows with
 // the product of row lengths); such matrices are treated as unsymmetric
 constexpr int64_t kSymmetryCheckMaxRow = 8192;

@@ -127,6 +127,7 @@ struct TraverseLaunch {
     int chunk;                  // consecutive sources per work item
     int merge;                  // 1: reuse the closures of reached cached sources
     int chain;                  // 1: start a source from the previous source's closure when it is known to hold
+    long long chain_wait_ns;    // wait this long for the other direction's result when it is one source behind
     int ring;                   // cached closures per CTA (power of 2, <= 64)
     long long sample_stride;    // > 1: process only every stride-th item (autotuner timing)
     long long bitmap_words;     // words per bitmap (covers max n + padding)

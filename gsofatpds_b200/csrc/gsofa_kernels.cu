@@ -941,10 +941,23 @@ __global__ void __launch_bounds__(BLOCK, 1024 / BLOCK) traverse_kernel(TraverseL
                 if (P.chain && P.bu_alpha <= 0 && nx < s_end) {
                     const int r0 = ld_i32<CG>(S.rp + nx), r1 = ld_i32<CG>(S.rp + nx + 1);
                     if ((r1 & ~3) - (r0 & ~3) <= kChainMaxRow) {
-                        if (lfold) ch = nbit;  // symmetric: U(src, src+1) = L(src+1, src)
-                        else if (M.link)
-                            ch = *reinterpret_cast<const volatile uint8_t*>(
-                                     M.link + 2ll * src + (1 - dir)) == 2;
+                        if (lfold) {
+                            ch = nbit;  // symmetric: U(src, src+1) = L(src+1, src)
+                        } else if (M.link) {
+                            const volatile uint8_t* lk = M.link + 2ll * src + (1 - dir);
+                            uint8_t v = *lk;
+                            // the other direction's search of this chunk has
+                            // finished src - 1 and is on src: wait a bounded
+                            // time for it rather than start src + 1 cold
+                            if (v == 0 && P.chain_wait_ns > 0 && src > s_first &&
+                                *(const volatile uint8_t*)(M.link + 2ll * (src - 1) + (1 - dir)) != 0) {
+                                const unsigned long long t0 = global_ns();
+                                while ((v = *lk) == 0 &&
+                                       global_ns() - t0 < (unsigned long long)P.chain_wait_ns)
+                                    __nanosleep(64);
+                            }
+                            ch = v == 2;
+                        }
                     }
                 }
                 SM.chain = ch;

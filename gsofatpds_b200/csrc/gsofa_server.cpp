@@ -182,15 +182,16 @@ size_t request_footprint(const gsofa_server* s, int32_t n, int64_t nnz) {
     return kept + staging + result_bytes(n, s->opts.flags);
 }
 
-// Consecutive sources per work item: the plain path's default for this
-// order and grid, capped so that chunk * n stays near 2^26 -- one item of a
+// Consecutive sources per work item: about four items per CTA for this
+// order and grid (requests share the CTAs, so items stay shorter than the
+// plain path's), capped so that chunk * n stays near 2^26 -- one item of a
 // large request then holds its CTA for milliseconds, not for a large part of
 // the request, and a request that arrives meanwhile finds CTAs soon.
 int request_chunk(const gsofa_server* s, int32_t n) {
     if (s->opts.chunk_sources > 0) return s->opts.chunk_sources;
     long long cap = 512;
     while (cap > 16 && cap * (long long)std::max(n, 1) > (1ll << 26)) cap >>= 1;
-    return (int)std::min<long long>(default_chunk(2ll * n, s->grid), cap);
+    return (int)std::min<long long>(default_chunk(2ll * n, 4 * s->grid), cap);
 }
 
 // Marks a request finished (done or failed) and releases its slot and memory.
@@ -362,6 +363,7 @@ bool launch_kernel(gsofa_server* s, int k, int grid) {
     L.chunk = 1;
     L.merge = s->merge ? 1 : 0;
     L.chain = s->merge && !(s->opts.flags & GSOFA_NO_CHAIN) ? 1 : 0;
+    L.chain_wait_ns = chain_wait_ns(s->opts);
     L.ring = s->ring;
     L.sample_stride = 1;
     L.bitmap_words = s->words;

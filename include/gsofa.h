@@ -89,7 +89,12 @@ typedef struct gsofa_opts {
     /* closures of recently finished sources each CTA keeps for reuse
      * (rounded down to a power of 2, at most 64); 0 = default */
     int32_t cached_closures;
-    int32_t reserved[2];
+    /* how long (microseconds) a source search may wait, when the search of
+     * the same chunk in the other direction is one source behind, for the
+     * result that lets it start from the previous source's closure; 0 =
+     * default, < 0 = never wait */
+    int32_t chain_wait_us;
+    int32_t reserved;
 } gsofa_opts;
 
 /* Defaults: max_supernode_size 128, autotuned CTA size, GPU-filling

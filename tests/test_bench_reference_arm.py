@@ -33,14 +33,21 @@ def test_reference_arm_without_a_counterpart_is_unavailable():
 
 
 def test_roofline_entry():
+    """The roofline object is the hardware one: measured DRAM bytes per
+    launch over the kernel time, as a fraction of the measured peak; the
+    algorithmic (work-equivalent) rate is reported beside it, not as frac."""
     sys.path.insert(0, ROOT)
     import bench
-    # config 2's numbers: E_alg, V_alg, n, kernel ms, measured peak, ncu bytes per launch
-    r = bench.roofline_entry(1316542257033, 148212479438, 659033, 871.76, 6456.2, "measured",
-                             548526653696.0)
-    assert r["bytes_alg"] == 8 * 1316542257033 + 16 * 148212479438 + 4 * 11 * 659033
+    # config 2's numbers: E_alg, V_alg, edges inspected, n, kernel ms, peak, ncu bytes per launch
+    r = bench.roofline_entry(1316542257033, 148212479438, 63747717944, 659033, 871.76, 6456.2,
+                             "measured", 548526653696.0)
+    assert r["bound"] == "hbm" and r["unit"] == "GB/s"
+    assert abs(r["achieved"] - 548526653696.0 / 0.87176 / 1e9) < 1e-6
     assert abs(r["frac"] - r["achieved"] / 6456.2) < 1e-12
-    assert abs(r["traffic_achieved"] - 548526653696.0 / 0.87176 / 1e9) < 1e-6
-    assert 0.09 < r["traffic_frac"] < 0.11
-    r0 = bench.roofline_entry(10, 1, 5, 1.0, 100.0, "fallback", None)
-    assert r0["traffic"] is None and "traffic_frac" not in r0
+    assert 0.09 < r["frac"] < 0.11
+    we = r["work_equivalent"]
+    assert we["bytes_alg"] == 8 * 1316542257033 + 16 * 148212479438 + 4 * 11 * 659033
+    assert we["gbs"] > r["peak"]  # closure reuse: not a bandwidth fraction
+    assert abs(r["inspected_edges_per_s"] - 63747717944 / 0.87176) < 1.0
+    r0 = bench.roofline_entry(10, 1, 4, 5, 1.0, 100.0, "fallback", None)
+    assert r0["traffic"] is None and r0["achieved"] is None and r0["frac"] is None
