@@ -96,12 +96,12 @@ size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
 
 long long bitmap_words(int32_t n) { return (((long long)n + 31) >> 5) + 6; }
 
-// Default chunk (consecutive sources per work item): about one chunk per
-// CTA, a power of 2 between 16 and 512 sources.  Each chunk's first source
-// starts cold (nothing to reuse), while later ones mostly start from their
-// predecessor's closure, so long chunks pay; the autotuner tries shorter
-// ones for matrices whose costly sources cluster (nested-dissection orders
-// put them in the top separators).
+// Default chunk (consecutive sources per work item): total / grid, a power
+// of 2 between 16 and 512 sources, where total weighs each matrix by
+// chunk_weight -- about one item per CTA for unsymmetric patterns.  Each
+// chunk's first source starts cold (nothing to reuse), while later ones
+// mostly start from their predecessor's closure, so long chunks pay; the
+// autotuner tries shorter and longer ones.
 long long default_chunk(long long total_sources, int grid) {
     long long c = total_sources / (grid > 0 ? grid : 1);
     long long p = 16;
@@ -109,7 +109,7 @@ long long default_chunk(long long total_sources, int grid) {
     return p;
 }
 
-long long work_sources(gsofa_ctx* ctx, const gsofa_matrix* m) {
+long long chunk_weight(gsofa_ctx* ctx, const gsofa_matrix* m) {
     if (m->host_sym < 0) {
         int sym = 0;
         if (m->n > 0 &&
@@ -121,7 +121,7 @@ long long work_sources(gsofa_ctx* ctx, const gsofa_matrix* m) {
             cudaGetLastError();
         m->host_sym = sym;
     }
-    return (m->host_sym ? 1ll : 2ll) * m->n;
+    return m->host_sym ? m->n / 4 : 2ll * m->n;
 }
 
 // Default CTA size: about 1024 resident threads per SM (the kernel is held
@@ -193,11 +193,11 @@ void result_free(gsofa_result* r) {
 }
 
 // Layout of a result arena: the per-row arrays of an n-row matrix.
-static size_t result_layout(int32_t n, uint32_t flags, size_t off[11]) {
+static size_t result_layout(int32_t n, uint32_t flags, size_t off[12]) {
     const size_t N = (size_t)std::max(n, 1);
     const bool dig = flags & GSOFA_DIGESTS;
     const bool lrow = flags & GSOFA_L_ROW_STATS;
-    size_t sz[11];
+    size_t sz[12];
     sz[0] = 4 * N;                       // nnz_u
     sz[1] = 4 * N;                       // nz_row_u
     sz[2] = dig ? 8 * N : 0;             // dig_u
@@ -209,8 +209,9 @@ static size_t result_layout(int32_t n, uint32_t flags, size_t off[11]) {
     sz[8] = N;                           // supernode flags
     sz[9] = 8 * CNT_SLOTS;               // counters
     sz[10] = 2 * N;                      // link (chained starts)
+    sz[11] = 16 * N;                     // umask (chained starts)
     size_t total = 0;
-    for (int i = 0; i < 11; i++) {
+    for (int i = 0; i < 12; i++) {
         off[i] = total;
         total += align256(sz[i]);
     }
@@ -218,7 +219,7 @@ static size_t result_layout(int32_t n, uint32_t flags, size_t off[11]) {
 }
 
 size_t result_bytes(int32_t n, uint32_t flags) {
-    size_t off[11];
+    size_t off[12];
     return result_layout(n, flags, off);
 }
 
@@ -234,7 +235,7 @@ int result_alloc_on(gsofa_ctx* ctx, int32_t n, uint32_t flags, int32_t mss, cuda
     const size_t N = (size_t)std::max(n, 1);
     const bool dig = flags & GSOFA_DIGESTS;
     const bool lrow = flags & GSOFA_L_ROW_STATS;
-    size_t off[11];
+    size_t off[12];
     const size_t total = result_layout(n, flags, off);
     int rc = dev_alloc_on(ctx, total, &r->arena, stream);
     if (rc) {
@@ -254,6 +255,7 @@ int result_alloc_on(gsofa_ctx* ctx, int32_t n, uint32_t flags, int32_t mss, cuda
     r->sflags = reinterpret_cast<int8_t*>(b + off[8]);
     r->counters = reinterpret_cast<unsigned long long*>(b + off[9]);
     r->link = reinterpret_cast<uint8_t*>(b + off[10]);
+    r->umask = reinterpret_cast<uint32_t*>(b + off[11]);
     // zero the scatter targets, the counters and the flags
     cudaError_t e = cudaSuccess;
     if (lrow) {
@@ -303,6 +305,7 @@ MatDesc make_desc(const gsofa_matrix* m, const gsofa_result* r, long long base) 
     d.lptr = r->lptr;
     d.lrows = r->lrows;
     d.link = r->link;
+    d.umask = r->umask;
     d.item_base = base;
     return d;
 }
@@ -316,7 +319,7 @@ int run_factor(gsofa_ctx* ctx, const gsofa_matrix* const* mats, int32_t count,
     long long total_sources = 0;
     for (int32_t i = 0; i < count; i++) {
         nmax = std::max(nmax, mats[i]->n);
-        total_sources += work_sources(ctx, mats[i]);
+        total_sources += chunk_weight(ctx, mats[i]);
     }
     LaunchCfg cfg;
     int rc = plan_launch(ctx, std::max(nmax, 1), o, &cfg);
@@ -926,7 +929,7 @@ static int autotune_impl(gsofa_ctx* ctx, const gsofa_matrix* const* mats, int32_
     if (cudaSetDevice(ctx->device) != cudaSuccess) return set_err(ctx, GSOFA_ERR_CUDA, "cudaSetDevice");
     for (int32_t i = 0; i < count; i++) {
         nmax = std::max(nmax, mats[i]->n);
-        total_sources += work_sources(ctx, mats[i]);
+        total_sources += chunk_weight(ctx, mats[i]);
     }
     gsofa_opts base = *opts;
     base.flags &= ~(uint32_t)(GSOFA_SUPERNODES | GSOFA_PATTERN | GSOFA_L_ROW_STATS);
@@ -1135,7 +1138,7 @@ int gsofa_batch_create(gsofa_ctx* ctx, const gsofa_matrix* const* mats, int32_t 
         nmax = std::max(nmax, mats[i]->n);
     }
     if (cudaSetDevice(ctx->device) != cudaSuccess) return set_err(ctx, GSOFA_ERR_CUDA, "cudaSetDevice");
-    for (int32_t i = 0; i < count; i++) total_sources += work_sources(ctx, mats[i]);
+    for (int32_t i = 0; i < count; i++) total_sources += chunk_weight(ctx, mats[i]);
     gsofa_batch* b = new (std::nothrow) gsofa_batch();
     if (!b) return set_err(ctx, GSOFA_ERR_OOM_BUDGET, "host allocation failed");
     b->ctx = ctx;

@@ -78,6 +78,7 @@ struct gsofa_result {
     int8_t* sflags = nullptr;
     unsigned long long* counters = nullptr;
     uint8_t* link = nullptr;  // 2n: chained-start links between the directions
+    uint32_t* umask = nullptr;  // 4n: U(f, f+1+j) bits, read by chained starts
     // pattern (separate allocation, only with GSOFA_PATTERN)
     void* parena = nullptr;
     size_t pbytes = 0;
@@ -132,10 +133,13 @@ int dev_alloc_on(gsofa_ctx* ctx, size_t bytes, void** p, cudaStream_t stream);
 void dev_free_on(gsofa_ctx* ctx, void* p, size_t bytes, cudaStream_t stream);
 size_t align256(size_t x);
 long long default_chunk(long long total_sources, int grid);
-// Source searches a factorization of m runs: n for a symmetric pattern (the
-// U-row searches fill both halves), else 2n.  Reads the ingest's symmetry
-// word back once (synchronous on ctx->stream) and keeps it with m.
-long long work_sources(gsofa_ctx* ctx, const gsofa_matrix* m);
+// m's share in the default chunk length: 2n for an unsymmetric pattern (a
+// U-row and an L-column search per source), n/4 for a symmetric one (the
+// U-row searches fill both halves, and its costly sources cluster in the top
+// separators of a nested-dissection order, which shorter chunks spread over
+// more CTAs).  Reads the ingest's symmetry word back once (synchronous on
+// ctx->stream) and keeps it with m.
+long long chunk_weight(gsofa_ctx* ctx, const gsofa_matrix* m);
 int default_block(int32_t nmax, int smem_per_sm);
 // Result arrays of an n-row matrix, zero-initialised on `stream`.
 int result_alloc_on(gsofa_ctx* ctx, int32_t n, uint32_t flags, int32_t mss, cudaStream_t stream,

@@ -59,6 +59,7 @@ struct MatDesc {
     int32_t* nnz_lc;            // n: |L column|
     uint64_t* dig_lc;           // n (or null)
     uint32_t* lmask;            // 4n: L(f+1+j, f) bits
+    uint32_t* umask;            // 4n or null: U(f, f+1+j) bits (read by chained starts)
     int8_t* sflags;             // n: supernode flags (batched supernode kernel)
     int32_t* nnz_lr;            // n or null (L row scatter)
     uint64_t* dig_lr;           // n or null

@@ -128,6 +128,7 @@ struct TraverseSmem {
     int ring_lo[64];      // per ring slot: the words its closure occupies
     int ring_hi[64];
     int chain;            // the next source starts from this source's bitmap
+    int premerge;         // else: ring slot of a cached source the next one is known to reach
 };
 
 // Bitmap words of a matrix of order n: n bits plus zero padding read by the
@@ -564,6 +565,43 @@ __device__ __forceinline__ unsigned long long global_ns() {
     return t;
 }
 
+// Called by the 32 lanes of warp 0 when source nx = src + 1 cannot start
+// from src's closure: the ring slot of the largest cached source t < src that
+// nx is known to reach, or -1.  nx reaches t when the other direction's
+// search of t has finished (its link byte is set) and its mask of
+// t+1 .. t+128 has bit nx: L(nx, t) != 0 for a U-row search (the L-column
+// mask of t), U(t, nx) != 0 for an L-column search (the U-row mask of t).  A
+// symmetric pattern reads bit nx of t's own closure in the ring.  Lane k
+// tests t = src - 1 - k (and t - 32).
+__device__ int premerge_candidate(const Src& S, const MatDesc& M, int32_t src, int32_t s_first,
+                                  int dir, bool lfold) {
+    const int lane = threadIdx.x & 31;
+    const int32_t nx = src + 1;
+    const int32_t lo = max(s_first, nx - S.ring);
+    for (int k0 = 0; k0 < 64; k0 += 32) {
+        const int32_t t = src - 1 - k0 - lane;
+        bool ok = false;
+        if (t >= lo) {
+            const int j = nx - t - 1;  // 1 .. 63: bit of nx in t's mask
+            if (lfold) {
+                const int slot = t & (S.ring - 1);
+                const int w = nx >> 5;
+                if (w >= S.ring_lo[slot] && w <= S.ring_hi[slot])
+                    ok = (S.ring_base[(long long)slot * S.words + w] >> (nx & 31)) & 1u;
+            } else if (M.link) {
+                uint32_t lk;
+                asm volatile("ld.acquire.gpu.global.u8 %0, [%1];"
+                             : "=r"(lk) : "l"(M.link + 2ll * t + (1 - dir)) : "memory");
+                const uint32_t* mk = dir == 0 ? M.lmask : M.umask;
+                if (lk != 0 && mk) ok = (__ldcg(mk + 4ll * t + (j >> 5)) >> (j & 31)) & 1u;
+            }
+        }
+        const unsigned b = __ballot_sync(FULL_MASK, ok);
+        if (b) return (src - 1 - k0 - (__ffs(b) - 1)) & (S.ring - 1);
+    }
+    return -1;
+}
+
 // Serving, called by all 32 lanes of warp 0: claims a work item of any
 // published request.  Each lane checks one list entry (rotating start); the
 // claimable entry with the fewest unclaimed items is taken with
@@ -710,7 +748,10 @@ __global__ void __launch_bounds__(BLOCK, 1024 / BLOCK) traverse_kernel(TraverseL
     } else if (threadIdx.x == 0) {
         SM.cta = blockIdx.x;
     }
-    if (threadIdx.x == 0) SM.chain = 0;
+    if (threadIdx.x == 0) {
+        SM.chain = 0;
+        SM.premerge = -1;
+    }
     const long long cta = MODE == 2 ? SM.cta : blockIdx.x;
     uint32_t* const sbm = reinterpret_cast<uint32_t*>(dyn_smem);
     uint32_t* const gbm = MODE == 1 ? nullptr : P.gbitmap + cta * P.bitmap_words;
@@ -809,7 +850,9 @@ __global__ void __launch_bounds__(BLOCK, 1024 / BLOCK) traverse_kernel(TraverseL
             S.cache_lo = P.merge ? max(s_first, src - P.ring) : src;
             S.merged_mask = 0ull;
             S.top = -1;
-            S.pending = 0ull;
+            // a cached source known (from the other direction's search) to be
+            // reached: merged right after the source's own row
+            S.pending = (P.merge && src > s_first && SM.premerge >= 0) ? (1ull << SM.premerge) : 0ull;
             S.reached = &SM.reached[0];
             S.qmark = 0;
             // the bitmap still holds the closure of src - 1 (decided by its census)
@@ -929,52 +972,64 @@ __global__ void __launch_bounds__(BLOCK, 1024 / BLOCK) traverse_kernel(TraverseL
                 atomicMin(&SM.wlo, wl);
                 atomicMax(&SM.whi, wh);
             }
-            if (threadIdx.x == 0) {
-                // src + 1 in this closure: publish it for the other direction's
-                // search of src + 1, then decide whether src + 1 chains (the
-                // search is over: every bit is final after its last barrier)
+            if (warp == 0) {
+                // Publish, for the other direction's searches, the 128 bits
+                // src+1 .. src+128 of this closure (lanes 0-3: the L-column
+                // mask of a direction-1 or symmetric search, the U-row mask
+                // of a direction-0 one) and then the link byte of src; then
+                // decide how src + 1 starts.  The search is over: every bit
+                // is final after its last barrier.
                 const int32_t nx = src + 1;
                 const bool nbit = nx < n && ((ld_vol(bm + (nx >> 5)) >> (nx & 31)) & 1u);
-                if (M.link && !lfold && !P.pattern_pass)
+                if (!P.pattern_pass && lane < 4) {
+                    const long long p = (long long)src + 1 + 32 * lane;
+                    const long long wd = p >> 5;
+                    const int off = (int)(p & 31);
+                    uint32_t val = bm[wd] >> off;
+                    if (off) val |= bm[wd + 1] << (32 - off);
+                    if (dir == 1 || lfold) M.lmask[4ll * src + lane] = val;
+                    else if (M.umask) M.umask[4ll * src + lane] = val;
+                    __threadfence();  // the masks are visible before the link
+                }
+                __syncwarp();
+                if (lane == 0 && M.link && !lfold && !P.pattern_pass)
                     *reinterpret_cast<volatile uint8_t*>(M.link + 2ll * src + dir) = nbit ? 2 : 1;
-                int ch = 0;
+                int ch = 0, pre = -1;
                 if (P.chain && P.bu_alpha <= 0 && nx < s_end) {
-                    const int r0 = ld_i32<CG>(S.rp + nx), r1 = ld_i32<CG>(S.rp + nx + 1);
-                    if ((r1 & ~3) - (r0 & ~3) <= kChainMaxRow) {
-                        if (lfold) {
-                            ch = nbit;  // symmetric: U(src, src+1) = L(src+1, src)
-                        } else if (M.link) {
-                            const volatile uint8_t* lk = M.link + 2ll * src + (1 - dir);
-                            uint8_t v = *lk;
-                            // the other direction's search of this chunk has
-                            // finished src - 1 and is on src: wait a bounded
-                            // time for it rather than start src + 1 cold
-                            if (v == 0 && P.chain_wait_ns > 0 && src > s_first &&
-                                *(const volatile uint8_t*)(M.link + 2ll * (src - 1) + (1 - dir)) != 0) {
-                                const unsigned long long t0 = global_ns();
-                                while ((v = *lk) == 0 &&
-                                       global_ns() - t0 < (unsigned long long)P.chain_wait_ns)
-                                    __nanosleep(64);
+                    if (lane == 0) {
+                        const int r0 = ld_i32<CG>(S.rp + nx), r1 = ld_i32<CG>(S.rp + nx + 1);
+                        if ((r1 & ~3) - (r0 & ~3) <= kChainMaxRow) {
+                            if (lfold) {
+                                ch = nbit;  // symmetric: U(src, src+1) = L(src+1, src)
+                            } else if (M.link) {
+                                const volatile uint8_t* lk = M.link + 2ll * src + (1 - dir);
+                                uint8_t v = *lk;
+                                // the other direction's search of this chunk has
+                                // finished src - 1 and is on src: wait a bounded
+                                // time for it rather than start src + 1 cold
+                                if (v == 0 && P.chain_wait_ns > 0 && src > s_first &&
+                                    *(const volatile uint8_t*)(M.link + 2ll * (src - 1) + (1 - dir)) != 0) {
+                                    const unsigned long long t0 = global_ns();
+                                    while ((v = *lk) == 0 &&
+                                           global_ns() - t0 < (unsigned long long)P.chain_wait_ns)
+                                        __nanosleep(64);
+                                }
+                                ch = v == 2;
                             }
-                            ch = v == 2;
                         }
                     }
+                    ch = __shfl_sync(FULL_MASK, ch, 0);
+                    if (!ch && P.merge) pre = premerge_candidate(S, M, src, s_first, dir, lfold);
                 }
-                SM.chain = ch;
+                if (lane == 0) {
+                    SM.chain = ch;
+                    SM.premerge = pre;
+                }
             }
             __syncthreads();
             const long long wlo = SM.wlo, whi = SM.whi;
             const bool chain_next = SM.chain != 0;
 
-            if ((dir == 1 || lfold) && !P.pattern_pass && threadIdx.x < 4) {
-                // 128-bit mask of rows f+1 .. f+128 in L column f (supernode test)
-                const long long p = (long long)src + 1 + 32 * threadIdx.x;
-                const long long wd = p >> 5;
-                const int off = (int)(p & 31);
-                uint32_t val = bm[wd] >> off;
-                if (off) val |= bm[wd + 1] << (32 - off);
-                M.lmask[4ll * src + threadIdx.x] = val;
-            }
             if (P.pattern_pass) {
                 // sorted ids of the set bits > src: U row (dir 0) or L column (dir 1)
                 int32_t* out = dir == 0 ? M.ucols : M.lrows;

@@ -184,13 +184,14 @@ size_t request_footprint(const gsofa_server* s, int32_t n, int64_t nnz) {
 
 // Consecutive sources per work item: about four items per CTA for this
 // order and grid (requests share the CTAs, so items stay shorter than the
-// plain path's), capped so that chunk * n stays near 2^26 -- one item of a
-// large request then holds its CTA for milliseconds, not for a large part of
-// the request, and a request that arrives meanwhile finds CTAs soon.
+// plain path's), capped so that chunk * n stays near 2^28 -- one item of a
+// large request then holds its CTA for a bounded time, not for a large part
+// of the request, and a request that arrives meanwhile finds CTAs soon.  The
+// cap is no tighter because every item's first source starts cold.
 int request_chunk(const gsofa_server* s, int32_t n) {
     if (s->opts.chunk_sources > 0) return s->opts.chunk_sources;
     long long cap = 512;
-    while (cap > 16 && cap * (long long)std::max(n, 1) > (1ll << 26)) cap >>= 1;
+    while (cap > 16 && cap * (long long)std::max(n, 1) > (1ll << 28)) cap >>= 1;
     return (int)std::min<long long>(default_chunk(2ll * n, 4 * s->grid), cap);
 }
 
