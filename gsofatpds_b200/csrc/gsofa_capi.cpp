@@ -109,6 +109,17 @@ long long default_chunk(long long total_sources, int grid) {
     return p;
 }
 
+// Launch order of a batch's matrices: most entries first (longest processing
+// time first), so that the persistent kernel's last items are small ones and
+// no large matrix starts when the rest of the batch is almost done.
+std::vector<int32_t> batch_order(const gsofa_matrix* const* mats, int32_t count) {
+    std::vector<int32_t> order((size_t)count);
+    for (int32_t i = 0; i < count; i++) order[(size_t)i] = i;
+    std::stable_sort(order.begin(), order.end(),
+                     [&](int32_t a, int32_t b) { return mats[a]->nnz > mats[b]->nnz; });
+    return order;
+}
+
 long long chunk_weight(gsofa_ctx* ctx, const gsofa_matrix* m) {
     if (m->host_sym < 0) {
         int sym = 0;
@@ -342,11 +353,13 @@ int run_factor(gsofa_ctx* ctx, const gsofa_matrix* const* mats, int32_t count,
                     (size_t)cfg.grid * (size_t)ring * (size_t)cfg.words * 4);
         if (rc) return rc;
     }
-    // matrix descriptors
+    // matrix descriptors, largest matrices first
+    const std::vector<int32_t> order = batch_order(mats, count);
     std::vector<MatDesc> descs((size_t)count);
     long long base = 0;
-    for (int32_t i = 0; i < count; i++) {
-        descs[i] = make_desc(mats[i], res[i], base);
+    for (int32_t k = 0; k < count; k++) {
+        const int32_t i = order[(size_t)k];
+        descs[(size_t)k] = make_desc(mats[i], res[i], base);
         base += 2ll * ((mats[i]->n + chunk - 1) / chunk);
     }
     void* ddesc = nullptr;
@@ -404,7 +417,8 @@ int run_factor(gsofa_ctx* ctx, const gsofa_matrix* const* mats, int32_t count,
 
     // pattern pass (second traversal writing sorted ids)
     if (o->flags & GSOFA_PATTERN) {
-        for (int32_t i = 0; i < count; i++) {
+        for (int32_t k = 0; k < count; k++) {
+            const int32_t i = order[(size_t)k];
             gsofa_result* r = res[i];
             CK(cudaMemcpyAsync(ctx->h_counters, r->counters, 8 * CNT_SLOTS, cudaMemcpyDeviceToHost,
                                ctx->stream));
@@ -426,7 +440,7 @@ int run_factor(gsofa_ctx* ctx, const gsofa_matrix* const* mats, int32_t count,
             if (rc) return rc;
             CK(launch_pattern_ptrs(r->n, r->nnz_u, r->nnz_lc, r->uptr, r->lptr, ctx->scan_tmp,
                                    ctx->scan_tmp_bytes, ctx->stream));
-            descs[i] = make_desc(mats[i], r, descs[i].item_base);
+            descs[(size_t)k] = make_desc(mats[i], r, descs[(size_t)k].item_base);
         }
         CK(cudaMemcpyAsync(ddesc, descs.data(), sizeof(MatDesc) * (size_t)count,
                            cudaMemcpyHostToDevice, ctx->stream));
@@ -983,7 +997,7 @@ static int autotune_impl(gsofa_ctx* ctx, const gsofa_matrix* const* mats, int32_
         if (plan_launch(ctx, nmax, &base, &c0) == GSOFA_OK) best.threads_per_source = c0.block;
         ctx->err.clear();
     }
-    const int tps_c[] = {256, 512, 1024};
+    const int tps_c[] = {128, 256, 512, 1024};
     for (int tps : tps_c) {
         if (tps == best.threads_per_source) continue;
         gsofa_opts p = best;
@@ -1167,10 +1181,12 @@ int gsofa_batch_create(gsofa_ctx* ctx, const gsofa_matrix* const* mats, int32_t 
     std::vector<MatDesc> descs((size_t)count);
     std::vector<long long> seg((size_t)count + 1, 0);
     long long base = 0;
-    for (int32_t i = 0; i < count; i++) {
-        descs[(size_t)i] = make_desc(mats[i], b->res[(size_t)i], base);
+    const std::vector<int32_t> order = batch_order(mats, count);  // largest first
+    for (int32_t k = 0; k < count; k++) {
+        const int32_t i = order[(size_t)k];
+        descs[(size_t)k] = make_desc(mats[i], b->res[(size_t)i], base);
         base += 2ll * ((mats[i]->n + chunk - 1) / chunk);
-        seg[(size_t)i + 1] = seg[(size_t)i] + supernode_segment_count(mats[i]->n, o.max_supernode_size);
+        seg[(size_t)k + 1] = seg[(size_t)k] + supernode_segment_count(mats[i]->n, o.max_supernode_size);
     }
     b->items = base;
     const size_t sz_small = 256;
@@ -1198,7 +1214,8 @@ int gsofa_batch_create(gsofa_ctx* ctx, const gsofa_matrix* const* mats, int32_t 
     uint32_t* dring = merge ? reinterpret_cast<uint32_t*>(p) : nullptr;
     p += sz_ring;
     uint32_t* dgbm = cfg.smem_bitmap ? nullptr : reinterpret_cast<uint32_t*>(p);
-    for (int32_t i = 0; i < count; i++) descs[(size_t)i].counters = dcnt + (size_t)i * CNT_SLOTS;
+    for (int32_t k = 0; k < count; k++)  // matrix i's counters at slot i, whatever its launch order
+        descs[(size_t)k].counters = dcnt + (size_t)order[(size_t)k] * CNT_SLOTS;
     cudaError_t e;
     if ((e = cudaMemcpyAsync(ddesc, descs.data(), sizeof(MatDesc) * (size_t)count,
                              cudaMemcpyHostToDevice, ctx->stream)) != cudaSuccess ||
