@@ -12,7 +12,9 @@
 // as one group of one chunk on one GPU of one node (N_GPU_Node = 1), which
 // is how the kernel reads a chunk: only the chunk's own rows and the markers
 // L(r, f) with f in the chunk.  The markers are scattered into a zeroed
-// mss x n array before the launch and cleared after it.
+// mss x n array before the launch and cleared after it.  The running
+// supernode counter carries over from launch to launch, and the kernel
+// indexes its supernode records with it, so those hold one entry per row.
 //
 // Input (binary, little-endian): int32 n, int32 mss, int32 nz_row_U[n],
 // int64 lptr[n+1], int32 lcols[lptr[n]] (the strictly-lower columns of each
@@ -85,7 +87,9 @@ int main(int argc, char** argv) {
     CK(cudaMemset(d_per_chunk, 0, sizeof(int) * n_chunks));
     CK(cudaMalloc(&d_dummy, sizeof(int) * 16));
     CK(cudaMemset(d_dummy, 0, sizeof(int) * 16));
-    CK(cudaMalloc(&d_super, sizeof(Super) * (size_t)(mss + 1)));
+    // the kernel stores supernode i at superObj_d[i], i from its running Nsup
+    // counter, which every launch continues: at most one per row in total
+    CK(cudaMalloc(&d_super, sizeof(Super) * ((size_t)n + 1)));
     long long cap = 1;
     long long *d_idx = nullptr;
     int* d_val = nullptr;
