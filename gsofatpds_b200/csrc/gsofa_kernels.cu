@@ -116,6 +116,8 @@ struct TraverseSmem {
     long long item;
     int cnt[3];
     int grab[3];          // per level (rotating): 32-vertex chunks of the frontier taken
+    int redo[3];          // per level (rotating): smallest queue index of a chunk abandoned
+                          // when a cached source was reached (INT_MAX: none)
     int abort_level;  // set when a cached source is reached: stop, merge, redo
     int pushed;       // ids a merge appended to the queue
     rmask_t pending;      // cached sources a merge set (slots), for the next decision
@@ -277,7 +279,7 @@ __device__ __forceinline__ unsigned td_edge4(const Src& S, int v, const int4& e,
 // are skipped: their reach is already in the bitmap.
 template <int BLOCK, bool CG>
 __device__ __forceinline__ void td_level(const Src& S, int32_t* q, long long qcap, long long lb,
-                                         long long le, int* cnt, int* grab, int32_t* status,
+                                         long long le, int* cnt, int* grab, int* redo, int32_t* status,
                                          int heavy_len, uint32_t& raw, uint32_t& orig,
                                          uint32_t& trav, int& wl, int& wh) {
     constexpr int NW = BLOCK / 32;
@@ -306,7 +308,13 @@ __device__ __forceinline__ void td_level(const Src& S, int32_t* q, long long qca
         nv = (nbase + lane < le) ? q[nbase + lane] : S.src;
         // stop when a cached source was reached; one value for the whole warp
         const int ab = __shfl_sync(FULL_MASK, *(volatile int*)S.abort_flag, 0);
-        if (lb > 0 && ab) break;
+        if (lb > 0 && ab) {
+            // chunks are handed out in increasing order and each is either
+            // finished or abandoned: the level is redone from the smallest
+            // abandoned one (this chunk; the prefetched next one is larger)
+            if (lane == 0) atomicMin(redo, (int)base);
+            break;
+        }
         int s0 = 0, plen = 0;
         if (i < le) {
             bool skip = false;
@@ -328,11 +336,14 @@ __device__ __forceinline__ void td_level(const Src& S, int32_t* q, long long qca
             const int hb = __shfl_sync(FULL_MASK, s0, l);
             const int hl = __shfl_sync(FULL_MASK, plen, l);
             const int hv = __shfl_sync(FULL_MASK, v, l);
+            // the next 128 entries are loaded before these are processed
+            int4 he = 4 * lane < hl ? ld_row4<CG>(S.cl + hb + 4 * lane) : idle;
             for (int k0 = 0; k0 < hl; k0 += 128) {
-                const int k = k0 + 4 * lane;
-                const int4 e = k < hl ? ld_row4<CG>(S.cl + hb + k) : idle;
-                const unsigned f = td_edge4(S, hv, e, raw, orig, wl, wh);
-                push4(q, qcap, le, cnt, status, lane, e, f);
+                const int kn = k0 + 128 + 4 * lane;
+                const int4 hn = kn < hl ? ld_row4<CG>(S.cl + hb + kn) : idle;
+                const unsigned f = td_edge4(S, hv, he, raw, orig, wl, wh);
+                push4(q, qcap, le, cnt, status, lane, he, f);
+                he = hn;
             }
         }
         if (plen > heavy_len) plen = 0;
@@ -864,6 +875,7 @@ __global__ void __launch_bounds__(BLOCK, 1024 / BLOCK) traverse_kernel(TraverseL
                 q[0] = src;
                 SM.cnt[0] = 0;
                 SM.grab[0] = 0;
+                SM.redo[0] = INT_MAX;
                 SM.reached[0] = 0ull;
                 SM.abort_level = 0;
                 if (S.chained) {  // the census range covers the kept bits too
@@ -893,11 +905,12 @@ __global__ void __launch_bounds__(BLOCK, 1024 / BLOCK) traverse_kernel(TraverseL
                     if (threadIdx.x == 0) {
                         SM.cnt[(level + 1) % 3] = 0;
                         SM.grab[(level + 1) % 3] = 0;
+                        SM.redo[(level + 1) % 3] = INT_MAX;
                         SM.reached[(level + 1) % 3] = 0ull;
                     }
                     S.reached = &SM.reached[level % 3];
                     td_level<BLOCK, CG>(S, q, qcap, lb, le, &SM.cnt[level % 3], &SM.grab[level % 3],
-                                        P.status, P.heavy_len, raw, orig, trav, wl, wh);
+                                        &SM.redo[level % 3], P.status, P.heavy_len, raw, orig, trav, wl, wh);
                     __syncthreads();
                     const int nxt = SM.cnt[level % 3];
                     level++;
@@ -916,7 +929,11 @@ __global__ void __launch_bounds__(BLOCK, 1024 / BLOCK) traverse_kernel(TraverseL
                         __syncthreads();
                         const int np = did ? SM.pushed : 0;
                         S.pending = did ? (SM.pending & ~mm) : (S.pending & ~mm);
-                        le = le + nxt + np;  // redo this level (it may have been cut short)
+                        // redo this level from its first abandoned chunk (every
+                        // earlier chunk was expanded; none abandoned: all were)
+                        const int rf = SM.redo[(level - 1) % 3];
+                        lb = rf < le ? (long long)rf : le;
+                        le = le + nxt + np;
                         S.qmark = (int)le;   // later entries are outside the merged closures
                     } else {
                         lb = le;
