@@ -586,9 +586,49 @@ void gsofa::host::ingest_bytes(int32_t n, int64_t nnz, size_t* kept, size_t* sta
                align256(canonicalize_scan_bytes(n)) + 256;
 }
 
+cudaError_t gsofa::host::PinnedStager::init() {
+    for (int k = 0; k < kBufs; k++) {
+        cudaError_t e = cudaHostAlloc(&buf[k], kPiece, cudaHostAllocDefault);
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ev[k], cudaEventDisableTiming);
+        if (e != cudaSuccess) return e;
+    }
+    return cudaSuccess;
+}
+
+void gsofa::host::PinnedStager::release() {
+    for (int k = 0; k < kBufs; k++) {
+        if (ev[k]) cudaEventSynchronize(ev[k]);
+        if (buf[k]) cudaFreeHost(buf[k]);
+        if (ev[k]) cudaEventDestroy(ev[k]);
+        buf[k] = nullptr;
+        ev[k] = nullptr;
+    }
+}
+
+cudaError_t gsofa::host::PinnedStager::upload(void* dst, const void* src, size_t bytes,
+                                              cudaStream_t stream) {
+    const char* p = static_cast<const char*>(src);
+    char* d = static_cast<char*>(dst);
+    while (bytes > 0) {
+        const size_t k = std::min(bytes, kPiece);
+        // the buffer's previous DMA is complete before it is refilled
+        cudaError_t e = cudaEventSynchronize(ev[next]);
+        if (e != cudaSuccess) return e;
+        std::memcpy(buf[next], p, k);
+        e = cudaMemcpyAsync(d, buf[next], k, cudaMemcpyHostToDevice, stream);
+        if (e == cudaSuccess) e = cudaEventRecord(ev[next], stream);
+        if (e != cudaSuccess) return e;
+        next = (next + 1) % kBufs;
+        p += k;
+        d += k;
+        bytes -= k;
+    }
+    return cudaSuccess;
+}
+
 int gsofa::host::ingest_csr(gsofa_ctx* ctx, cudaStream_t stream, int32_t* dstatus, int32_t n,
                             int64_t nnz, const int32_t* row_begin, const int32_t* row_end,
-                            const int32_t* col, gsofa_matrix** out) {
+                            const int32_t* col, gsofa_matrix** out, PinnedStager* stager) {
     *out = nullptr;
     if (n < 0 || nnz < 0) return set_err(ctx, GSOFA_ERR_ARG, "negative n or nnz");
     if (n > 0 && (!row_begin || !row_end)) return set_err(ctx, GSOFA_ERR_ARG, "null row arrays");
@@ -627,11 +667,13 @@ int gsofa::host::ingest_csr(gsofa_ctx* ctx, cudaStream_t stream, int32_t* dstatu
     if (rc) { matrix_free_on(m, stream); return rc; }
     int32_t* dbeg = reinterpret_cast<int32_t*>(sblk);
     int32_t* dcol_in = reinterpret_cast<int32_t*>(reinterpret_cast<char*>(sblk) + align256(4 * N1));
-    cudaError_t e = cudaMemcpyAsync(m->rowptr, rp.data(), 4 * N1, cudaMemcpyHostToDevice, stream);
-    if (e == cudaSuccess && n > 0)
-        e = cudaMemcpyAsync(dbeg, row_begin, 4 * (size_t)n, cudaMemcpyHostToDevice, stream);
-    if (e == cudaSuccess && nnz > 0)
-        e = cudaMemcpyAsync(dcol_in, col, 4 * (size_t)nnz, cudaMemcpyHostToDevice, stream);
+    auto up = [&](void* dst, const void* src, size_t bytes) {
+        return stager ? stager->upload(dst, src, bytes, stream)
+                      : cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, stream);
+    };
+    cudaError_t e = up(m->rowptr, rp.data(), 4 * N1);
+    if (e == cudaSuccess && n > 0) e = up(dbeg, row_begin, 4 * (size_t)n);
+    if (e == cudaSuccess && nnz > 0) e = up(dcol_in, col, 4 * (size_t)nnz);
     if (e != cudaSuccess) {
         dev_free_on(ctx, sblk, stage, stream);
         matrix_free_on(m, stream);

@@ -147,13 +147,29 @@ int result_alloc_on(gsofa_ctx* ctx, int32_t n, uint32_t flags, int32_t mss, cuda
 void result_free(gsofa_result* r);
 void supernodal_free(gsofa_result* r);  // caller holds ctx->mu
 MatDesc make_desc(const gsofa_matrix* m, const gsofa_result* r, long long base);
+// Uploads from pageable host memory through a few pinned buffers: the host
+// copies the next piece into one buffer while the previous piece's DMA
+// runs, and no upload waits for the stream's earlier work to finish (a
+// pageable cudaMemcpyAsync synchronises its stream first).  One caller at a
+// time; upload() returns once the source may be reused.
+struct PinnedStager {
+    static constexpr int kBufs = 4;
+    static constexpr size_t kPiece = 8u << 20;
+    void* buf[kBufs] = {};
+    cudaEvent_t ev[kBufs] = {};
+    int next = 0;
+    cudaError_t init();
+    void release();
+    cudaError_t upload(void* dst, const void* src, size_t bytes, cudaStream_t stream);
+};
 // Validates the row intervals on the host, then queues the upload and the
 // padded-CSR build of A and A^T on `stream` without waiting.  Column ids
 // outside [0, n) are reported in *dstatus (DEV_ERR_COL_RANGE) when the
-// stream reaches the build.  The caller holds ctx->mu.
+// stream reaches the build.  The caller holds ctx->mu.  With `stager` the
+// host arrays are uploaded through it (see PinnedStager), else directly.
 int ingest_csr(gsofa_ctx* ctx, cudaStream_t stream, int32_t* dstatus, int32_t n, int64_t nnz,
                const int32_t* row_begin, const int32_t* row_end, const int32_t* col,
-               gsofa_matrix** out);
+               gsofa_matrix** out, PinnedStager* stager = nullptr);
 // A matrix handle and its device block for n rows, `real` entries and
 // `padded` padded entries of A (rows rounded up to multiples of 4).
 int matrix_alloc(gsofa_ctx* ctx, cudaStream_t stream, int32_t n, int64_t real, int64_t padded,

@@ -85,6 +85,7 @@ constexpr int kReserveSms = 4;
 constexpr long long kMaxIdlePolls = 1000000;  // a cap far above idle_ns worth of polls
 constexpr long long kIdleNs = 300000;         // a CTA with nothing to claim for 0.3 ms exits
 constexpr double kTopUpCheckMs = 0.5;         // how often a partial launch is topped up
+constexpr double kAdmitSliceMs = 1.0;         // admissions per loop pass stop after this long
 constexpr size_t kDefaultBudget = 40ull << 30;
 constexpr double kShutdownGraceMs = 120000.0;  // destroy waits this long for queued work
 
@@ -136,6 +137,8 @@ struct gsofa_server {
     unsigned long long* h_claim = nullptr;
     unsigned long long* h_cnt = nullptr;
     int32_t* h_sstat = nullptr;
+    // uploads of the submitted (pageable) host arrays
+    gsofa::host::PinnedStager stager;
     // host state (mu guards everything a caller thread touches)
     std::mutex mu;
     std::condition_variable cv_work, cv_done;
@@ -304,7 +307,7 @@ bool admit_one(gsofa_server* s) {
         std::lock_guard<std::recursive_mutex> g(ctx->mu);
         if (rc == GSOFA_OK)
             rc = ingest_csr(ctx, s->as, s->d_slot_status + slot, r->n, r->nnz, r->beg, r->end,
-                            r->col, &r->mat);
+                            r->col, &r->mat, &s->stager);
         if (rc == GSOFA_OK)
             rc = result_alloc_on(ctx, r->n, flags, s->opts.max_supernode_size, s->as, &r->res);
         if (rc != GSOFA_OK) why = ctx->err;
@@ -538,7 +541,14 @@ void loop(gsofa_server* s) {
     double shutdown_at = -1.0;
     for (;;) {
         bool progress = false;
-        while (admit_one(s)) progress = true;
+        // admit in slices, so that publication, the kernel launch and the
+        // read-back of finished requests are not held up behind the uploads
+        // of a long queue
+        const double t_adm = now_ms(s);
+        while (admit_one(s)) {
+            progress = true;
+            if (now_ms(s) - t_adm > kAdmitSliceMs) break;
+        }
         // requests whose claim word is on the device and whose items are not
         // all finished
         bool claimable = false;
@@ -634,6 +644,7 @@ void release(gsofa_server* s) {
     if (s->h_claim) cudaFreeHost(s->h_claim);
     if (s->h_cnt) cudaFreeHost(s->h_cnt);
     if (s->h_sstat) cudaFreeHost(s->h_sstat);
+    s->stager.release();
 }
 
 }  // namespace
@@ -737,7 +748,8 @@ int gsofa_server_create(gsofa_ctx* ctx, const gsofa_opts* opts, int32_t max_n,
     if ((e = cudaMallocHost((void**)&s->h_desc, sizeof(MatDesc) * kSlots)) != cudaSuccess ||
         (e = cudaMallocHost((void**)&s->h_claim, 8 * kSlots)) != cudaSuccess ||
         (e = cudaMallocHost((void**)&s->h_cnt, 8 * CNT_SLOTS * kSlots)) != cudaSuccess ||
-        (e = cudaMallocHost((void**)&s->h_sstat, 4 * kSlots)) != cudaSuccess)
+        (e = cudaMallocHost((void**)&s->h_sstat, 4 * kSlots)) != cudaSuccess ||
+        (e = s->stager.init()) != cudaSuccess)
         return fail(GSOFA_ERR_CUDA, "pinned host memory", e);
 
     // device workspace: per-CTA queues, closure rings and global bitmaps
