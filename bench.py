@@ -46,6 +46,9 @@ WORKLOADS = {
     "steal": "the 512-matrix batch mix as 32 chunks of 16 matrices spread over the ranks by "
              "longest-first per-rank queues with work stealing; each claimed chunk is one batched "
              "launch (shape from gsofa_autotune_batch)",
+    "reference_build": "the matrices the reference's own CUDA build (SpaceOptimization, unmodified, "
+                       "sm_100a) was timed on: BC n=11948, n=20000 random, 64^3 ND grid, circuit-like "
+                       "n=20000, banded, grid and small raw-layout patterns",
     "serve": "Poisson request stream, n log-uniform [1000, 1000000], 5-27 nnz/row: 2D 5/9-point and "
              "3D 7/27-point ND grids, random-banded unsymmetric (n capped), 40 GB budget, mss 128",
 }
@@ -225,6 +228,66 @@ def run_reference(args, rank, world):
                                             "nnz": int(rp[-1]), "mss": mss},
             "cpu_baseline": cb,
             "e2e": {"value": v, "unit": "GTEPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def run_reference_build(args, local):
+    """Beside the reference's own CUDA build on the same GPU model: the fill
+    detection times that the unmodified SPO binary's own timer reported
+    (symbfact.cuh:2004, :2420), recorded by tests/golden/make_reference_spo.py
+    in tests/golden/reference_spo.json, against this library's plain
+    factorization of the same matrices (device time, CUDA events on the
+    launching stream, L2 flushed, library defaults, supernodes included).
+    Each matrix's fill count is checked against the reference's."""
+    import torch
+    from gsofatpds_b200 import Context
+    from tests import reference_inputs as RI
+    recs = json.load(open(os.path.join(ROOT, "tests", "golden", "reference_spo.json")))["records"]
+    torch.cuda.set_device(local)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    rows = []
+    with Context(local) as ctx:
+        stream = torch.cuda.Stream()
+        torch.cuda.set_stream(stream)
+        ctx.set_stream(stream.cuda_stream)
+        for label, rec in sorted(recs.items()):
+            if not rec.get("ms_reference"):
+                continue
+            beg, end, col = RI.build(label)
+            m = ctx.load_csr(beg, end, col)
+            for _ in range(args.warmup):
+                ctx.factor(m, max_supernode_size=128).close()
+            ts, fills = [], None
+            for _ in range(args.steps):
+                flush.zero_()
+                e0 = torch.cuda.Event(enable_timing=True)
+                e1 = torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                r = ctx.factor(m, max_supernode_size=128)
+                e1.record(stream)
+                torch.cuda.synchronize()
+                ts.append(e0.elapsed_time(e1))
+                fills = r.counts["fill_count"]
+                r.close()
+            m.close()
+            if fills != rec["fills_reference"]:
+                raise SystemExit("%s: fills %d, the reference build printed %d" %
+                                 (label, fills, rec["fills_reference"]))
+            ms = float(np.median(ts))
+            rows.append({"input": label, "n": rec["n"], "nnz": rec["nnz"],
+                         "virtual_gpus": rec["virtual_gpus"], "memory_gb": rec["memory_gb"],
+                         "ms_reference_build": rec["ms_reference"], "ms": ms,
+                         "speedup": rec["ms_reference"] / ms, "fills": fills})
+    sp = [r["speedup"] for r in rows]
+    line = {"metric": "speedup_vs_reference_build", "unit": "x",
+            "value": float(np.exp(np.mean(np.log(sp)))) if sp else None,
+            "value_kind": "geometric mean over the inputs of the reference build's own fill-detection "
+                          "time / this library's device time",
+            "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
+            "dtype": "int32", "data": "synthetic and the reference's BC matrix",
+            "config": {"workload": WORKLOADS["reference_build"],
+                       "l2": "flushed (256 MB write) before every timed step"},
+            "rows": rows}
     print(json.dumps(line), flush=True)
 
 
@@ -720,6 +783,9 @@ def main():
         return
     if args.workload == "order":
         run_order(args, local)
+        return
+    if args.workload == "reference_build":
+        run_reference_build(args, local)
         return
     if args.workload == "steal":
         run_steal(args, rank, world, local)

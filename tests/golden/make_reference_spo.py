@@ -2,14 +2,16 @@
 (oracle/_ref/spo_symbfact, `make -C oracle ref` in a checkout with the
 reference tree) on a GPU machine over the matrices of
 tests/reference_inputs.py, after oracle/ref_spo.check has cleared each input
-and pool size, and writes the fill counts it prints to
-tests/golden/reference_spo.json.  tests/test_reference_spo.py then checks the
-oracle against them on the CPU.
+and pool size, and writes the fill counts it prints, with the time its own
+timer reports for the fill detection, to tests/golden/reference_spo.json.
+tests/test_reference_spo.py then checks the oracle against them on the CPU;
+bench.py --workload reference_build times this library on the same inputs.
 
 Usage (GPU machine): python tests/golden/make_reference_spo.py [label ...]
 """
 import json
 import os
+import re
 import sys
 import time
 
@@ -37,9 +39,14 @@ def main():
         t0 = time.time()
         fills, out = ref_spo.run(beg, end, col, v, gb, timeout=spec.get("timeout", 600))
         dt = time.time() - t0
-        tail = [ln for ln in out.splitlines() if ln.startswith(("vertex count", "Total Number"))]
+        tail = [ln.strip() for ln in out.splitlines()
+                if ln.strip().startswith(("vertex count", "Total Number", "GPU:"))]
+        # the reference's own timer around its fill detection (symbfact.cuh:2004, :2420),
+        # printed per virtual GPU (:2530); with one virtual GPU, the whole run
+        m = re.search(r"Slowest virtual GPU takes: ([0-9.eE+-]+) ms", out)
         recs[label] = {"n": len(beg), "nnz": len(col), "virtual_gpus": v, "memory_gb": gb,
-                       "fills_reference": fills, "seconds": round(dt, 2), "printed": tail}
+                       "fills_reference": fills, "seconds": round(dt, 2), "printed": tail,
+                       "ms_reference": float(m.group(1)) if m else None}
         print(label, len(beg), fills, "%.1f s" % dt, flush=True)
         with open(out_path, "w") as f:
             json.dump({"generator": "tests/golden/make_reference_spo.py",
