@@ -44,7 +44,7 @@ EXPORTS = [
     "gsofa_server_wait", "gsofa_server_ticket_info", "gsofa_server_get_stats",
     "gsofa_server_destroy", "gsofa_server_last_error", "gsofa_autotune_batch",
     "gsofa_write_csr_binary", "gsofa_read_csr_binary", "gsofa_convert_dat_to_binary",
-    "gsofa_load_csr_binary", "gsofa_result_supernodal", "gsofa_order_nd", "gsofa_matrix_permute",
+    "gsofa_load_csr_binary", "gsofa_result_supernodal", "gsofa_order_nd", "gsofa_order_hybrid", "gsofa_matrix_permute",
     "gsofa_order_wait_selftest",
 ]
 
@@ -141,6 +141,7 @@ def load():
         "gsofa_result_supernodal": [vp, ctypes.POINTER(i64), ctypes.POINTER(i64), ctypes.POINTER(i64),
                                     vp, vp, vp, vp, vp],
         "gsofa_order_nd": [vp, vp, i32, i32, vp, ctypes.POINTER(OrderStats)],
+        "gsofa_order_hybrid": [vp, vp, i32, vp, ctypes.POINTER(OrderStats)],
         "gsofa_matrix_permute": [vp, vp, vp, ctypes.POINTER(vp)],
         "gsofa_order_wait_selftest": [vp, ctypes.c_double],
         "gsofa_batch_create": [vp, ctypes.POINTER(vp), i32, ctypes.POINTER(Opts), ctypes.POINTER(vp)],

@@ -149,6 +149,18 @@ class Context:
         stats = {f: getattr(st, f) for f, _ in C.OrderStats._fields_ if f != "reserved"}
         return perm[:n], stats
 
+    def order_hybrid(self, mat, leaf_size=0):
+        """Fill-reducing ordering of A + A^T by hybrid nested dissection
+        (level-set and multilevel separators, the smaller kept at each
+        split), computed on the device.  Returns (perm, stats) as order_nd."""
+        n = mat.n
+        perm = np.zeros(max(n, 1), np.int32)
+        st = C.OrderStats()
+        self._check(self._L.gsofa_order_hybrid(self._h, mat.handle, int(leaf_size), _ptr(perm),
+                                               ctypes.byref(st)), "order_hybrid")
+        stats = {f: getattr(st, f) for f, _ in C.OrderStats._fields_ if f != "reserved"}
+        return perm[:n], stats
+
     def permute(self, mat, perm):
         """P A P^T on the device: row k is row perm[k] of `mat`, columns renamed."""
         p = np.ascontiguousarray(perm, dtype=np.int32)

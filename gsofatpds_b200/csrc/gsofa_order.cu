@@ -51,6 +51,7 @@
 #include <vector>
 
 #include "gsofa_host.h"
+#include "gsofa_order_ml.h"
 
 using namespace gsofa;
 using namespace gsofa::host;
@@ -520,16 +521,44 @@ __global__ void separator_kernel(Graph g, int32_t n, const int32_t* __restrict__
     }
 }
 
+// The hybrid rule's choice per part (pml[k] = 1: the multilevel split).  A
+// multilevel split is used when its separator is smaller than the level-set
+// one and leaves both sides non-empty.
+__global__ void choose_kernel(int R, const int32_t* __restrict__ psize, int32_t leaf,
+                              const int32_t* __restrict__ pcnts, const int32_t* __restrict__ pns,
+                              const int32_t* __restrict__ pna, const int32_t* __restrict__ pnb,
+                              int32_t* __restrict__ pml) {
+    for (long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x; k < R;
+         k += (long long)gridDim.x * blockDim.x)
+        pml[k] = psize[k] > leaf && pns[k] < pcnts[k] && pna[k] > 0 && pnb[k] > 0 ? 1 : 0;
+}
+
+// The split of each part: S placed last in its range, A and B become parts 2k
+// and 2k + 1 of the next round.  Level-set split: S = the separator flags on
+// level m, A = the rest of levels <= m; multilevel (pml[k]): S = msep, A and B
+// by mside.
 __global__ void assign_kernel(int32_t n, int32_t* __restrict__ part,
                               const int32_t* __restrict__ dist, const int32_t* __restrict__ pm,
                               const int32_t* __restrict__ sflag, const int32_t* __restrict__ plo,
                               const int32_t* __restrict__ psize, const int32_t* __restrict__ pcnts,
-                              unsigned long long* __restrict__ fkey) {
+                              unsigned long long* __restrict__ fkey, const int32_t* __restrict__ pml,
+                              const int32_t* __restrict__ mside, const int32_t* __restrict__ msep,
+                              const int32_t* __restrict__ pns) {
     for (long long vv = (long long)blockIdx.x * blockDim.x + threadIdx.x; vv < n;
          vv += (long long)gridDim.x * blockDim.x) {
         const int v = (int)vv;
         const int k = part[v];
         if (k < 0) continue;
+        if (pml && pml[k]) {
+            if (msep[v]) {
+                const int slo = plo[k] + psize[k] - pns[k];
+                fkey[v] = ((unsigned long long)(uint32_t)slo << 32) | (uint32_t)v;
+                part[v] = -1;
+            } else {
+                part[v] = 2 * k + mside[v];
+            }
+            continue;
+        }
         const int d = dist[v], m = pm[k];
         if (d == m && sflag[v]) {
             const int slo = plo[k] + psize[k] - pcnts[k];
@@ -548,13 +577,15 @@ __global__ void next_parts_kernel(int R, const int32_t* __restrict__ psize, int3
                                   const int32_t* __restrict__ plo, const int32_t* __restrict__ pa0,
                                   const int32_t* __restrict__ pnm,
                                   const int32_t* __restrict__ pcnts, int32_t* __restrict__ plo_next,
-                                  unsigned long long* tot) {
+                                  unsigned long long* tot, const int32_t* __restrict__ pml,
+                                  const int32_t* __restrict__ pns, const int32_t* __restrict__ pna) {
     for (long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x; k < R;
          k += (long long)gridDim.x * blockDim.x) {
         const int size = psize[k];
         if (size <= leaf) continue;
-        const int s = pcnts[k];
-        const int a = pa0[k] + pnm[k] - s;
+        const bool ml = pml && pml[k];
+        const int s = ml ? pns[k] : pcnts[k];
+        const int a = ml ? pna[k] : pa0[k] + pnm[k] - s;
         plo_next[2 * k] = plo[k];
         plo_next[2 * k + 1] = plo[k] + a;
         atomicAdd(tot + 0, (unsigned long long)(size - s));
@@ -616,7 +647,7 @@ int bits_for(long long x) {  // bits to hold values 0..x
 }
 
 int order_impl(gsofa_ctx* ctx, const gsofa_matrix* mat, int32_t leaf, int32_t max_rounds,
-               int32_t* perm, gsofa_order_stats* stats) {
+               bool hybrid, int32_t* perm, gsofa_order_stats* stats) {
     const int32_t n = mat->n;
     cudaStream_t st = ctx->stream;
     DeviceScratch S(ctx);
@@ -661,6 +692,22 @@ int order_impl(gsofa_ctx* ctx, const gsofa_matrix* mat, int32_t leaf, int32_t ma
         !sflag || !s || !excl || !plo || !psize || !proot || !pr1 || !pecc || !pm || !pa0 ||
         !pnm || !pcnts || !plo_a || !plo_b || !dperm || !keys || !sorted || !fkey || !small || !tmp)
         return set_err(ctx, GSOFA_ERR_OOM_BUDGET, "ordering workspace exceeds the budget");
+    // the hybrid rule's multilevel splits (gsofa_order_ml.cu)
+    SymGraph Hg;
+    int32_t *mside = nullptr, *msep = nullptr, *pns = nullptr, *pna = nullptr, *pnb = nullptr,
+            *pml = nullptr;
+    if (hybrid) {
+        mside = i32(N);
+        msep = i32(N);
+        pns = i32(N);
+        pna = i32(N);
+        pnb = i32(N);
+        pml = i32(N);
+        if (!mside || !msep || !pns || !pna || !pnb || !pml)
+            return set_err(ctx, GSOFA_ERR_OOM_BUDGET, "ordering workspace exceeds the budget");
+        int rc = sym_graph_build(ctx, S, n, mat->rowptr, mat->col, mat->trowptr, mat->tcol, &Hg);
+        if (rc) return rc;
+    }
     int32_t* nroots = small;
     unsigned* bar = reinterpret_cast<unsigned*>(small + 8);
     int32_t* err = small + 10;
@@ -740,10 +787,17 @@ int order_impl(gsofa_ctx* ctx, const gsofa_matrix* mat, int32_t leaf, int32_t ma
                                                    pnm, err);
         cudaMemsetAsync(pcnts, 0, 4 * (size_t)std::max(R, 1), st);
         separator_kernel<<<GW, kThreads, 0, st>>>(g, n, part, dist, pm, sflag, pcnts);
-        assign_kernel<<<G, kThreads, 0, st>>>(n, part, dist, pm, sflag, plo, psize, pcnts, fkey);
+        if (hybrid) {
+            rc = ml_round(ctx, Hg, n, part, R, psize, leaf_eff, mside, msep, pns, pna, pnb);
+            if (rc) return rc;
+            choose_kernel<<<grid_for(R, kThreads), kThreads, 0, st>>>(R, psize, leaf_eff, pcnts,
+                                                                      pns, pna, pnb, pml);
+        }
+        assign_kernel<<<G, kThreads, 0, st>>>(n, part, dist, pm, sflag, plo, psize, pcnts, fkey,
+                                              pml, mside, msep, pns);
         cudaMemsetAsync(tot, 0, 32, st);
-        next_parts_kernel<<<grid_for(R, kThreads), kThreads, 0, st>>>(R, psize, leaf_eff, plo, pa0,
-                                                                      pnm, pcnts, plo_next, tot);
+        next_parts_kernel<<<grid_for(R, kThreads), kThreads, 0, st>>>(
+            R, psize, leaf_eff, plo, pa0, pnm, pcnts, plo_next, tot, pml, pns, pna);
         unsigned long long ht[4] = {0, 0, 0, 0};
         int32_t herr = 0;
         cudaError_t e = cudaGetLastError();  // launch errors of this round
@@ -794,7 +848,21 @@ extern "C" int gsofa_order_nd(gsofa_ctx* ctx, const gsofa_matrix* mat, int32_t l
     if (stats) *stats = gsofa_order_stats{};
     if (mat->n == 0) return GSOFA_OK;
     return order_impl(ctx, mat, leaf_size > 0 ? leaf_size : kDefaultLeaf,
-                      max_rounds > 0 ? max_rounds : kDefaultMaxRounds, perm, stats);
+                      max_rounds > 0 ? max_rounds : kDefaultMaxRounds, false, perm, stats);
+}
+
+extern "C" int gsofa_order_hybrid(gsofa_ctx* ctx, const gsofa_matrix* mat, int32_t leaf_size,
+                                  int32_t* perm, gsofa_order_stats* stats) {
+    if (!ctx || !mat || (mat->n > 0 && !perm)) return GSOFA_ERR_ARG;
+    if (mat->ctx != ctx) return set_err(ctx, GSOFA_ERR_ARG, "matrix belongs to another context");
+    std::lock_guard<std::recursive_mutex> lk(ctx->mu);
+    if (cudaSetDevice(ctx->device) != cudaSuccess)
+        return set_err(ctx, GSOFA_ERR_CUDA, "cudaSetDevice");
+    if (stats) *stats = gsofa_order_stats{};
+    if (mat->n == 0) return GSOFA_OK;
+    // no round cap: every round places at least one separator vertex
+    return order_impl(ctx, mat, leaf_size > 0 ? leaf_size : kDefaultLeaf, mat->n + 2, true, perm,
+                      stats);
 }
 
 extern "C" int gsofa_matrix_permute(gsofa_ctx* ctx, const gsofa_matrix* mat, const int32_t* perm,

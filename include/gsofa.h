@@ -167,6 +167,18 @@ typedef struct gsofa_order_stats {
  * every remaining component whole).  stats may be NULL. */
 int gsofa_order_nd(gsofa_ctx* ctx, const gsofa_matrix* mat, int32_t leaf_size, int32_t max_rounds,
                    int32_t* perm, gsofa_order_stats* stats);
+/* Hybrid nested dissection, on the device: gsofa_order_nd's rounds (no round
+ * cap), where every component to be cut also gets a multilevel bisection --
+ * coarsening by mutual heavy-edge proposals, BFS growth on the coarsest
+ * graph, boundary refinement at every level within 40..60 % balance -- and
+ * the boundary of its side with fewer boundary vertices is used as the
+ * separator when it is smaller than the level-set one and leaves both sides
+ * non-empty.  On small-world graphs (circuit-like patterns) level sets give
+ * very large separators and the multilevel ones cut the fill; on grids the
+ * level-set separator wins and is kept.  Deterministic: the same matrix
+ * always gives the same perm.  Arguments as gsofa_order_nd. */
+int gsofa_order_hybrid(gsofa_ctx* ctx, const gsofa_matrix* mat, int32_t leaf_size, int32_t* perm,
+                       gsofa_order_stats* stats);
 /* The symmetrically permuted matrix P A P^T built on the device: row k of
  * *out is row perm[k] of mat with every column id c renamed to the k' with
  * perm[k'] = c.  perm: host, n entries, a permutation of 0..n-1 (else

@@ -353,7 +353,51 @@ def test_grid_barrier_wait_runs_out_and_context_survives(ctx):
     m.close()
 
 
-# ---- the hybrid rule (oracle only; no device counterpart yet) --------------------
+# ---- the hybrid rule ---------------------------------------------------------------
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("leaf", [1, 8, 32])
+def test_device_hybrid_equals_oracle(ctx, leaf):
+    """gsofa_order_hybrid against or_order_hybrid: the same permutation and
+    the same statistics on every graph of the battery."""
+    for name, (b, e, c) in _cases().items():
+        m = ctx.load_csr(b, e, c)
+        perm, st = ctx.order_hybrid(m, leaf_size=leaf)
+        ref, rst = O.order_hybrid(b, e, c, leaf=leaf)
+        np.testing.assert_array_equal(perm, ref, err_msg="%s leaf %d" % (name, leaf))
+        assert (st["rounds"], st["splits"], st["separator_vertices"],
+                st["max_separator"]) == rst, (name, leaf, st, rst)
+        m.close()
+
+
+@pytest.mark.gpu
+def test_device_hybrid_circuit_like_and_grid():
+    """A circuit-like matrix (multilevel separators win) and an unscrambled
+    3D grid (coarsening stops at once: the whole-device BFS in queue order):
+    identical to the oracle, and the circuit-like fill is cut."""
+    _cuda()
+    from gsofatpds_b200 import Context, gen
+    from gsofatpds_b200.gen import csr_to_beg_end
+    _, rp, col = gen_circuit(30000)
+    b, e = csr_to_beg_end(rp)
+    _, grp, gcol = gen.grid_nd((32, 32, 32), "7")
+    gb, ge = csr_to_beg_end(grp)
+    got = {}
+    with Context(0) as c:
+        for name, (bb, ee, cc) in (("circuit30k", (b, e, col)), ("grid32", (gb, ge, gcol))):
+            m = c.load_csr(bb, ee, cc)
+            perm, st = c.order_hybrid(m, leaf_size=32)
+            ref, rst = O.order_hybrid(bb, ee, cc, leaf=32)
+            np.testing.assert_array_equal(perm, ref, err_msg=name)
+            assert (st["rounds"], st["splits"], st["separator_vertices"],
+                    st["max_separator"]) == rst, (name, st, rst)
+            got[name] = perm
+            m.close()
+    pl, _ = O.order_nd(b, e, col, leaf=32)
+    assert _fill(*permuted(b, e, col, got["circuit30k"])) < _fill(*permuted(b, e, col, pl))
+
+
+# ---- the hybrid rule's oracle -------------------------------------------------------
 
 @pytest.mark.parametrize("seed", range(12))
 def test_hybrid_oracle_is_a_deterministic_permutation(seed):
