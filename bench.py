@@ -40,7 +40,8 @@ WORKLOADS = {
               "binary CSR file and from host memory (upload, padded CSR of A and A^T, checks)",
     "handoff": "supernodal block form (gsofa_result_supernodal) of the n=20000 random matrix and the "
                "64^3 ND grid, from their materialised patterns, mss 128",
-    "order": "fill-reducing ordering (gsofa_order_nd, level-set nested dissection of A + A^T, leaf 32) "
+    "order": "fill-reducing ordering (gsofa_order_nd, level-set nested dissection of A + A^T, and "
+             "gsofa_order_hybrid, level-set or multilevel separator per split; leaf 32) "
              "of the 64^3 7-point grid under a seeded random symmetric permutation (n=262144), "
              "the n=20000 random matrix and the circuit-like n=659033 matrix",
     "steal": "the 512-matrix batch mix as 32 chunks of 16 matrices spread over the ranks by "
@@ -456,9 +457,11 @@ def run_handoff(args, local):
 
 
 def run_order(args, local):
-    """Ordering on the device against the oracle's single-thread ordering;
-    the fill of each ordered matrix is measured by factoring it on the
-    device (the 64^3 grid also against its coordinate-bisection ND order)."""
+    """Ordering on the device against the oracle's single-thread ordering,
+    for both rules (level-set nested dissection, gsofa_order_nd, and the
+    hybrid with multilevel separators, gsofa_order_hybrid); the fill of each
+    ordered matrix is measured by factoring it on the device (the 64^3 grid
+    also against its coordinate-bisection ND order)."""
     import torch
     from gsofatpds_b200 import Context, gen
     from gsofatpds_b200.gen import csr_to_beg_end
@@ -498,20 +501,43 @@ def run_order(args, local):
             ref, _ = O.order_nd(b, e, ccol)
             row["cpu_oracle_ms"] = (time.perf_counter() - t0) * 1e3
             row["equal_to_oracle"] = bool(np.array_equal(ref, perm))
-            if name != "circuit_like" or args.order_factor_all:
-                pm = ctx.permute(m, perm)
-                r = ctx.factor(pm)
-                row["fill_ordered"] = int(r.counts["fill_count"])
-                row["factor_ms_ordered"] = float(r.counts["ms_device"])
-                r.close()
-                pm.close()
+            pm = ctx.permute(m, perm)
+            r = ctx.factor(pm)
+            row["fill_ordered"] = int(r.counts["fill_count"])
+            row["factor_ms_ordered"] = float(r.counts["ms_device"])
+            r.close()
+            pm.close()
+            # the hybrid rule
+            hms, hwall = [], []
+            for it in range(1 + max(1, min(args.steps, 3))):
+                t0 = time.perf_counter()
+                hperm, hst = ctx.order_hybrid(m)
+                w = (time.perf_counter() - t0) * 1e3
+                if it >= 1:
+                    hms.append(hst["ms"])
+                    hwall.append(w)
+            hy = dict(ms_device=float(np.median(hms)), ms_call=float(np.median(hwall)),
+                      rounds=hst["rounds"], splits=hst["splits"],
+                      separator_vertices=hst["separator_vertices"],
+                      max_separator=hst["max_separator"])
+            t0 = time.perf_counter()
+            href, _ = O.order_hybrid(b, e, ccol)
+            hy["cpu_oracle_ms"] = (time.perf_counter() - t0) * 1e3
+            hy["equal_to_oracle"] = bool(np.array_equal(href, hperm))
+            pm = ctx.permute(m, hperm)
+            r = ctx.factor(pm)
+            hy["fill_ordered"] = int(r.counts["fill_count"])
+            hy["factor_ms_ordered"] = float(r.counts["ms_device"])
+            r.close()
+            pm.close()
+            row["hybrid"] = hy
             if nd_ref is not None:
                 m2 = ctx.load_rowptr(*nd_ref)
                 r = ctx.factor(m2)
                 row["fill_coordinate_nd"] = int(r.counts["fill_count"])
                 r.close()
                 m2.close()
-            elif name != "circuit_like" or args.order_factor_all:
+            else:
                 r = ctx.factor(m)
                 row["fill_given_order"] = int(r.counts["fill_count"])
                 r.close()
@@ -758,8 +784,6 @@ def main():
     ap.add_argument("--no-mix", action="store_true",
                     help="default workload: skip the batch (config 4) and serving (config 5) "
                          "measurements embedded in the line")
-    ap.add_argument("--order-factor-all", action="store_true",
-                    help="order workload: also factor the circuit-like matrix in both orders")
     args = ap.parse_args()
 
     rank = int(os.environ.get("RANK", "0"))

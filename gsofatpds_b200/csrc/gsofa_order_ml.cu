@@ -40,14 +40,18 @@
 //   coarse ids   an exclusive scan of the "pair's smaller member" flags;
 //   contraction  64-bit (coarse u, coarse w) keys radix-sorted with their
 //                weights and reduced by key: the coarse CSR, rows sorted;
-//   BFS order    level-synchronous over all parts, each new level sorted by
-//                (global queue position of the first parent, id): exactly the
-//                queue order of a sequential BFS that visits neighbours in
-//                id order;
+//   BFS order    parts of up to 256 vertices: one thread each, a plain
+//                sequential BFS; larger parts: one CTA each, level by level
+//                with block barriers, each new vertex appended by its first
+//                parent in queue order (the smallest queue position among its
+//                frontier neighbours) at an offset from a block scan, in
+//                adjacency order: exactly the queue order of a sequential BFS
+//                that visits neighbours in id order;
 //   refinement   gains and candidates one thread per vertex; candidates
 //                compacted in increasing id; then one thread per part
 //                accepts them in order against the balance bounds (the one
 //                sequential step; a pass has few candidates).
+#include <cub/block/block_scan.cuh>
 #include <cub/device/device_radix_sort.cuh>
 #include <cub/device/device_reduce.cuh>
 #include <cub/device/device_scan.cuh>
@@ -72,9 +76,9 @@ constexpr int kMatchRounds = 3;
 constexpr int kRefinePasses = 10;
 constexpr unsigned long long kNoKey = ~0ull;
 // parts of at most this many vertices are searched by one thread each (a
-// plain sequential BFS, all such parts at once); larger ones level by level
-// over the whole device
-constexpr int32_t kSeqBfsMax = 16384;
+// plain sequential BFS, all such parts at once); larger ones by one CTA each
+constexpr int32_t kSeqBfsMax = 256;
+constexpr int kCtaBfsThreads = 1024;
 
 int blocks_for(long long items) {
     long long g = (items + kT - 1) / kT;
@@ -291,97 +295,6 @@ __global__ void coarse_rows_kernel(long long m, const unsigned long long* __rest
 
 // ---- breadth-first search in exact queue order ---------------------------------
 
-// the start of each searched part: its queue holds the one vertex
-__global__ void bfs_start_kernel(int R, const int32_t* __restrict__ on,
-                                 const int32_t* __restrict__ start, const int32_t* __restrict__ pb,
-                                 int32_t* __restrict__ pos, int32_t* __restrict__ lev,
-                                 int32_t* __restrict__ qord, int32_t* __restrict__ cnt) {
-    GRID_LOOP(k, R) {
-        if (!on[k]) continue;
-        const int s = start[k];
-        pos[s] = 0;
-        lev[s] = 0;
-        qord[pb[k]] = s;
-        cnt[k] = 1;
-    }
-}
-
-__global__ void bfs_reset_kernel(long long V, const int32_t* __restrict__ vpart,
-                                 const int32_t* __restrict__ on, int32_t* __restrict__ pos,
-                                 int32_t* __restrict__ lev, int32_t* __restrict__ par) {
-    GRID_LOOP(x, V) {
-        pos[x] = -1;
-        lev[x] = on[vpart[x]] ? -1 : -2;  // -2: not searched
-        par[x] = INT_MAX;
-    }
-}
-
-// vertices on level `l` offer their global queue position to unvisited
-// neighbours; a neighbour keeps the smallest (its first parent in queue
-// order) and is listed once
-__global__ void bfs_expand_kernel(long long V, int l, const int32_t* __restrict__ xadj,
-                                  const int32_t* __restrict__ adj, const int32_t* __restrict__ vpart,
-                                  const int32_t* __restrict__ pb, const int32_t* __restrict__ lev,
-                                  const int32_t* __restrict__ pos, int32_t* par, int32_t* lst,
-                                  int32_t* lcount) {
-    GRID_LOOP(x, V) {
-        if (lev[x] != l) continue;
-        const int gp = pb[vpart[x]] + pos[x];
-        for (int j = xadj[x]; j < xadj[x + 1]; j++) {
-            const int y = adj[j];
-            if (lev[y] != -1) continue;
-            const int old = atomicMin(par + y, gp);
-            if (old == INT_MAX) lst[atomicAdd(lcount, 1)] = y;
-        }
-    }
-}
-
-__global__ void bfs_keys_kernel(int m, const int32_t* __restrict__ lst,
-                                const int32_t* __restrict__ par, unsigned long long* __restrict__ keys) {
-    GRID_LOOP(i, m) {
-        const int y = lst[i];
-        keys[i] = ((unsigned long long)(uint32_t)par[y] << 32) | (uint32_t)y;
-    }
-}
-
-// sorted new vertices: part k's are one run; each takes the next position
-__global__ void bfs_place_kernel(int m, int l, const unsigned long long* __restrict__ s,
-                                 const int32_t* __restrict__ vpart, const int32_t* __restrict__ pb,
-                                 const int32_t* __restrict__ cnt, int32_t* __restrict__ pos,
-                                 int32_t* __restrict__ lev, int32_t* __restrict__ qord,
-                                 int32_t* __restrict__ run_first) {
-    GRID_LOOP(i, m) {
-        const int y = (int)(uint32_t)s[i];
-        const int k = vpart[y];
-        if (i == 0 || vpart[(int)(uint32_t)s[i - 1]] != k) run_first[k] = (int)i;
-    }
-}
-
-__global__ void bfs_place2_kernel(int m, int l, const unsigned long long* __restrict__ s,
-                                  const int32_t* __restrict__ vpart, const int32_t* __restrict__ pb,
-                                  int32_t* __restrict__ cnt, int32_t* __restrict__ pos,
-                                  int32_t* __restrict__ lev, int32_t* __restrict__ qord,
-                                  const int32_t* __restrict__ run_first) {
-    GRID_LOOP(i, m) {
-        const int y = (int)(uint32_t)s[i];
-        const int k = vpart[y];
-        const int p = cnt[k] + (int)i - run_first[k];
-        pos[y] = p;
-        lev[y] = l + 1;
-        qord[pb[k] + p] = y;
-    }
-}
-
-__global__ void bfs_count_kernel(int m, const unsigned long long* __restrict__ s,
-                                 const int32_t* __restrict__ vpart,
-                                 const int32_t* __restrict__ run_first, int32_t* __restrict__ cnt) {
-    GRID_LOOP(i, m) {
-        const int y = (int)(uint32_t)s[i];
-        const int k = vpart[y];
-        if (i == m - 1 || vpart[(int)(uint32_t)s[i + 1]] != k) cnt[k] += (int)i - run_first[k] + 1;
-    }
-}
-
 // one thread per part: the sequential BFS from start[k], its queue in qord
 __global__ void seq_bfs_kernel(int R, const int32_t* __restrict__ on,
                                const int32_t* __restrict__ start, const int32_t* __restrict__ pb,
@@ -407,6 +320,80 @@ __global__ void seq_bfs_kernel(int R, const int32_t* __restrict__ on,
             }
         }
         cnt[k] = t;
+    }
+}
+
+// One CTA per part: the BFS from start[k] with its queue (qord) in exactly
+// the order a sequential BFS visiting neighbours in id order produces.  Per
+// level, every unvisited neighbour of the frontier keeps the smallest queue
+// position of a frontier vertex next to it (its first parent); each frontier
+// vertex counts the neighbours it won, a block scan over the frontier in
+// queue order gives each its offset, and it appends them in adjacency order.
+// Block barriers only; the loop ends when a level adds nothing.
+__global__ void __launch_bounds__(kCtaBfsThreads) cta_bfs_kernel(
+    int R, const int32_t* __restrict__ on, const int32_t* __restrict__ start,
+    const int32_t* __restrict__ pb, const int32_t* __restrict__ pn,
+    const int32_t* __restrict__ xadj, const int32_t* __restrict__ adj, int32_t* lev,
+    int32_t* par, int32_t* __restrict__ qord, int32_t* __restrict__ cnt) {
+    typedef cub::BlockScan<int, kCtaBfsThreads> Scan;
+    __shared__ typename Scan::TempStorage scan;
+    for (int k = blockIdx.x; k < R; k += gridDim.x) {
+        if (!on[k]) continue;
+        const int base = pb[k], size = pn[k];
+        for (int i = base + threadIdx.x; i < base + size; i += blockDim.x) {
+            lev[i] = -1;
+            par[i] = INT_MAX;
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            const int s = start[k];
+            qord[base] = s;
+            lev[s] = 0;
+        }
+        __syncthreads();
+        int h = 0, t = 1, level = 0;
+        while (h < t) {
+            for (int i = h + threadIdx.x; i < t; i += blockDim.x) {
+                const int u = qord[base + i];
+                for (int j = xadj[u]; j < xadj[u + 1]; j++) {
+                    const int y = adj[j];
+                    if (lev[y] == -1) atomicMin(par + y, i);
+                }
+            }
+            __syncthreads();
+            int tt = t;
+            for (int c0 = h; c0 < t; c0 += blockDim.x) {
+                const int i = c0 + threadIdx.x;
+                int mine = 0;
+                if (i < t) {
+                    const int u = qord[base + i];
+                    for (int j = xadj[u]; j < xadj[u + 1]; j++) {
+                        const int y = adj[j];
+                        mine += lev[y] == -1 && par[y] == i;
+                    }
+                }
+                int off = 0, total = 0;
+                Scan(scan).ExclusiveSum(mine, off, total);
+                if (i < t && mine) {
+                    const int u = qord[base + i];
+                    int o = tt + off;
+                    for (int j = xadj[u]; j < xadj[u + 1]; j++) {
+                        const int y = adj[j];
+                        if (lev[y] == -1 && par[y] == i && o < size) {
+                            qord[base + o++] = y;
+                            lev[y] = level + 1;
+                        }
+                    }
+                }
+                tt += total;
+                __syncthreads();  // scan storage reuse; this chunk's marks are visible
+            }
+            h = t;
+            t = tt < size ? tt : size;
+            level++;
+        }
+        if (threadIdx.x == 0) cnt[k] = t;
+        __syncthreads();
     }
 }
 
@@ -853,17 +840,14 @@ int ml_round(gsofa_ctx* ctx, const SymGraph& H, int32_t n, const int32_t* part, 
     int32_t* on_small = i32(R);
     int32_t* on_big = i32(R);
     int32_t* bcnt = i32(R);
-    int32_t* run_first = i32(R);
     int32_t* done = i32(R);
     int32_t* ccount = i32(R + 1);
     int32_t* cstart = i32(R + 1);
     int32_t* err = i32(2);
     long long* ptotal = i64(R);
     long long* pw0 = i64(R);
-    int32_t* pos = i32(V0);
     int32_t* lev = i32(V0);
     int32_t* par = i32(V0);
-    int32_t* lst = i32(V0);
     int32_t* qord = i32(V0);
     int32_t* gain = i32(V0);
     int32_t* cand = i32(V0);
@@ -871,11 +855,9 @@ int ml_round(gsofa_ctx* ctx, const SymGraph& H, int32_t n, const int32_t* part, 
     int32_t* nsel = i32(1);
     long long* wq = i64(V0 + 1);
     long long* wscan = i64(V0 + 1);
-    unsigned long long* bkeys = u64(V0);
-    unsigned long long* bsorted = u64(V0);
-    if (!start || !on || !on_small || !on_big || !bcnt || !run_first || !done || !ccount || !cstart || !err || !ptotal ||
-        !pw0 || !pos || !lev || !par || !lst || !qord || !gain || !cand || !clist || !nsel || !wq ||
-        !wscan || !bkeys || !bsorted)
+    if (!start || !on || !on_small || !on_big || !bcnt || !done || !ccount || !cstart || !err ||
+        !ptotal || !pw0 || !lev || !par || !qord || !gain || !cand || !clist || !nsel || !wq ||
+        !wscan)
         return fail(ctx, "bisection");
     cudaMemsetAsync(err, 0, 8, st);
     // queue slots of a part are all written by a search that covers it; the
@@ -887,37 +869,13 @@ int ml_round(gsofa_ctx* ctx, const SymGraph& H, int32_t n, const int32_t* part, 
 
     // one exact-order search of the parts flagged in `on` at level c, from
     // start[]: the small ones (on_small) one thread each, the others (on_big)
-    // level by level
-    auto bfs = [&](Level& c, bool big) -> int {
-        const long long V = c.V;
+    // one CTA each
+    auto bfs = [&](Level& c, int nbig) -> int {
         seq_bfs_kernel<<<blocks_for(R), kT, 0, st>>>(R, on_small, start, c.pb, c.pn, c.xadj, c.adj,
                                                      lev, qord, bcnt);
-        if (!big) {
-            bfs_check_kernel<<<blocks_for(R), kT, 0, st>>>(R, on, c.pn, bcnt, err);
-            return GSOFA_OK;
-        }
-        bfs_reset_kernel<<<blocks_for(V), kT, 0, st>>>(V, c.vpart, on_big, pos, lev, par);
-        bfs_start_kernel<<<blocks_for(R), kT, 0, st>>>(R, on_big, start, c.pb, pos, lev, qord, bcnt);
-        for (int l = 0;; l++) {
-            cudaMemsetAsync(cnt, 0, 4, st);
-            bfs_expand_kernel<<<blocks_for(V), kT, 0, st>>>(V, l, c.xadj, c.adj, c.vpart, c.pb, lev,
-                                                            pos, par, lst, cnt);
-            int32_t m = 0;
-            cudaMemcpyAsync(&m, cnt, 4, cudaMemcpyDeviceToHost, st);
-            if (int rc = sync("hybrid ordering: BFS")) return rc;
-            if (m == 0) break;
-            bfs_keys_kernel<<<blocks_for(m), kT, 0, st>>>(m, lst, par, bkeys);
-            size_t b = 0;
-            cub::DeviceRadixSort::SortKeys(nullptr, b, bkeys, bsorted, m, 0, 64, st);
-            if (!T.need(b)) return fail(ctx, "sort storage");
-            b = T.bytes;
-            cub::DeviceRadixSort::SortKeys(T.p, b, bkeys, bsorted, m, 0, 64, st);
-            bfs_place_kernel<<<blocks_for(m), kT, 0, st>>>(m, l, bsorted, c.vpart, c.pb, bcnt, pos,
-                                                           lev, qord, run_first);
-            bfs_place2_kernel<<<blocks_for(m), kT, 0, st>>>(m, l, bsorted, c.vpart, c.pb, bcnt, pos,
-                                                            lev, qord, run_first);
-            bfs_count_kernel<<<blocks_for(m), kT, 0, st>>>(m, bsorted, c.vpart, run_first, bcnt);
-        }
+        if (nbig > 0)
+            cta_bfs_kernel<<<std::min(nbig, 2 * ctx->sm_count), kCtaBfsThreads, 0, st>>>(
+                R, on_big, start, c.pb, c.pn, c.xadj, c.adj, lev, par, qord, bcnt);
         bfs_check_kernel<<<blocks_for(R), kT, 0, st>>>(R, on, c.pn, bcnt, err);
         return GSOFA_OK;
     };
@@ -933,14 +891,15 @@ int ml_round(gsofa_ctx* ctx, const SymGraph& H, int32_t n, const int32_t* part, 
         // parts whose coarsest level is this one: BFS growth
         cudaMemcpyAsync(hpn.data(), c.pn, 4 * (size_t)R, cudaMemcpyDeviceToHost, st);
         if (int rc = sync("hybrid ordering: part sizes")) return rc;
-        bool any = false, big = false;
+        bool any = false;
+        int nbig = 0;
         for (int k = 0; k < R; k++) {
             const size_t i = (size_t)k;
             hon[i] = hclev[i] == lv ? 1 : 0;
             hsmall[i] = hon[i] && hpn[i] <= kSeqBfsMax ? 1 : 0;
             hbig[i] = hon[i] && !hsmall[i] ? 1 : 0;
             any |= hon[i] != 0;
-            big |= hbig[i] != 0;
+            nbig += hbig[i];
         }
         cudaMemsetAsync(ptotal, 0, 8 * (size_t)R, st);
         part_weights_kernel<<<blocks_for(V), kT, 0, st>>>(V, c.vpart, c.vw, nullptr, ptotal, nullptr);
@@ -950,7 +909,7 @@ int ml_round(gsofa_ctx* ctx, const SymGraph& H, int32_t n, const int32_t* part, 
             cudaMemcpyAsync(on_big, hbig.data(), 4 * (size_t)R, cudaMemcpyHostToDevice, st);
             first_of_part_kernel<<<blocks_for(R), kT, 0, st>>>(R, on, c.pb, start);
             for (int rep_i = 0; rep_i < 3; rep_i++) {
-                if (int rc = bfs(c, big)) return rc;
+                if (int rc = bfs(c, nbig)) return rc;
                 if (rep_i < 2) last_of_queue_kernel<<<blocks_for(R), kT, 0, st>>>(R, on, c.pb, c.pn, qord, start);
             }
             queue_weights_kernel<<<blocks_for(V), kT, 0, st>>>(V, c.vpart, on, qord, c.pb, c.vw, wq);
@@ -982,13 +941,17 @@ int ml_round(gsofa_ctx* ctx, const SymGraph& H, int32_t n, const int32_t* part, 
             b = T.bytes;
             cub::DeviceSelect::Flagged(T.p, b, thrust::counting_iterator<int32_t>(0), cand, clist,
                                        nsel, (int)V, st);
-            cudaMemsetAsync(err + 1, 0, 4, st);
+            // parts that moved nothing are done and skip later passes; the
+            // host looks every other pass whether any part is left
+            if (pass % 2 == 0) cudaMemsetAsync(err + 1, 0, 4, st);
             accept_kernel<<<blocks_for(R), kT, 0, st>>>(R, cstart, ccount, clist, c.vw, ptotal, pw0,
                                                         c.side, done, err + 1);
-            int32_t moved = 0;
-            cudaMemcpyAsync(&moved, err + 1, 4, cudaMemcpyDeviceToHost, st);
-            if (int rc = sync("hybrid ordering: refinement")) return rc;
-            if (!moved) break;
+            if (pass % 2 == 1) {
+                int32_t moved = 0;
+                cudaMemcpyAsync(&moved, err + 1, 4, cudaMemcpyDeviceToHost, st);
+                if (int rc = sync("hybrid ordering: refinement")) return rc;
+                if (!moved) break;
+            }
         }
     }
 
