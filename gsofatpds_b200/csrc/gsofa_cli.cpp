@@ -7,9 +7,11 @@
 // Two more modes for the binary CSR files of include/gsofa.h:
 //   gsofa_cli --convert beg end csr out.gsofacsr   (parse once, no GPU)
 //   gsofa_cli --binary file.gsofacsr max_supernode_size
-// and one that orders the matrix on the device first (gsofa_order_nd, then
-// gsofa_matrix_permute) and factors the permuted matrix:
+// and two that order the matrix on the device first (gsofa_order_nd or
+// gsofa_order_hybrid, then gsofa_matrix_permute) and factor the permuted
+// matrix:
 //   gsofa_cli --order file.gsofacsr max_supernode_size
+//   gsofa_cli --order-hybrid file.gsofacsr max_supernode_size
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -17,7 +19,8 @@
 
 #include "../../include/gsofa.h"
 
-static int run_binary(const char* path, int mss, bool order) {
+// order: 0 = none, 1 = level-set nested dissection, 2 = hybrid
+static int run_binary(const char* path, int mss, int order) {
     gsofa_ctx* ctx = nullptr;
     int rc = gsofa_create(0, 0, &ctx);
     if (rc) {
@@ -37,12 +40,14 @@ static int run_binary(const char* path, int mss, bool order) {
         std::vector<int32_t> perm((size_t)n);
         gsofa_order_stats st;
         gsofa_matrix* pm = nullptr;
-        rc = gsofa_order_nd(ctx, m, 0, 0, perm.data(), &st);
+        rc = order == 2 ? gsofa_order_hybrid(ctx, m, 0, perm.data(), &st)
+                        : gsofa_order_nd(ctx, m, 0, 0, perm.data(), &st);
         if (rc == GSOFA_OK) rc = gsofa_matrix_permute(ctx, m, perm.data(), &pm);
         if (rc == GSOFA_OK) {
-            printf("Ordering (nested dissection on the device): %g ms, %d rounds, %lld separator "
+            printf("Ordering (%s nested dissection on the device): %g ms, %d rounds, %lld separator "
                    "vertices\n",
-                   st.ms, st.rounds, (long long)st.separator_vertices);
+                   order == 2 ? "hybrid" : "level-set", st.ms, st.rounds,
+                   (long long)st.separator_vertices);
             gsofa_matrix_destroy(m);
             m = pm;
         }
@@ -75,9 +80,10 @@ int main(int argc, char** argv) {
         }
         return 0;
     }
-    if (argc == 4 && strcmp(argv[1], "--binary") == 0)
-        return run_binary(argv[2], atoi(argv[3]), false);
-    if (argc == 4 && strcmp(argv[1], "--order") == 0) return run_binary(argv[2], atoi(argv[3]), true);
+    if (argc == 4 && strcmp(argv[1], "--binary") == 0) return run_binary(argv[2], atoi(argv[3]), 0);
+    if (argc == 4 && strcmp(argv[1], "--order") == 0) return run_binary(argv[2], atoi(argv[3]), 1);
+    if (argc == 4 && strcmp(argv[1], "--order-hybrid") == 0)
+        return run_binary(argv[2], atoi(argv[3]), 2);
     if (argc != 11 && argc != 6) {
         fprintf(stderr,
                 "usage: %s beg end csr #Processes max_supernode_size percent_cat0 percent_cat2 "
@@ -85,8 +91,9 @@ int main(int argc, char** argv) {
                 "   or: %s beg end csr N_virtualGPU total_memory_GB\n"
                 "   or: %s --convert beg end csr out.gsofacsr\n"
                 "   or: %s --binary file.gsofacsr max_supernode_size\n"
-                "   or: %s --order file.gsofacsr max_supernode_size\n",
-                argv[0], argv[0], argv[0], argv[0], argv[0]);
+                "   or: %s --order file.gsofacsr max_supernode_size\n"
+                "   or: %s --order-hybrid file.gsofacsr max_supernode_size\n",
+                argv[0], argv[0], argv[0], argv[0], argv[0], argv[0]);
         return 1;
     }
     printf("Number of Processes: %s\n", argv[4]);

@@ -89,6 +89,13 @@ int or_order_nd(int32_t n, const int32_t* beg, const int32_t* end, const int32_t
  * of the two used.  Same outputs as or_order_nd (no round cap). */
 int or_order_hybrid(int32_t n, const int32_t* beg, const int32_t* end, const int32_t* col,
                     int32_t leaf, int32_t* perm, int64_t* stats);
+/* or_order_hybrid, also recording every split in trace (7 int32 per split:
+ * range start, component size, |A|, |B|, |S|, rule 0 level-set / 1
+ * multilevel, the level-set separator's size), at most trace_cap splits;
+ * *trace_n gets the number of splits (which may exceed trace_cap). */
+int or_order_hybrid_trace(int32_t n, const int32_t* beg, const int32_t* end, const int32_t* col,
+                          int32_t leaf, int32_t* perm, int64_t* stats, int32_t* trace,
+                          int64_t trace_cap, int64_t* trace_n);
 
 /* Parse the reference's ASCII files (csr: "E N" then E ids; beg/end: n ids).
  * Allocates *beg,*end,*col with malloc; caller frees with or_free.

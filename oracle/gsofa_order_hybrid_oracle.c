@@ -1,7 +1,8 @@
 /*
  * gsofa_order_hybrid_oracle.c -- CPU oracle of the hybrid nested-dissection
- * rule (TEST INFRASTRUCTURE ONLY; libgsofa.so has no device counterpart of
- * this rule yet, and never links or calls this file).
+ * rule (TEST INFRASTRUCTURE ONLY: the checker of gsofa_order_hybrid, whose
+ * device implementation is gsofatpds_b200/csrc/gsofa_order.cu and
+ * gsofa_order_ml.cu; libgsofa.so never links or calls this file).
  *
  * The hybrid rule is or_order_nd's (gsofa_order_oracle.c) with one change at
  * each split: a second, multilevel separator is computed for the component,
@@ -326,7 +327,13 @@ typedef struct {
     int* loc;   /* local ids inside split(), -1 elsewhere */
     int* mark;  /* component walk of solve() */
     int64_t stats[4];
+    int32_t* trace;  /* or_order_hybrid_trace: kTraceFields per split, or NULL */
+    int64_t trace_cap, trace_n;
 } hctx;
+
+/* one split as traced: range start, component size, |A|, |B|, |S|, rule
+ * (0 level-set, 1 multilevel), and the level-set separator's size */
+enum { kTraceFields = 7 };
 
 static void place(hctx* H, int* vs, int k, int lo) {
     qsort(vs, (size_t)k, sizeof(int), cmp_i);
@@ -367,6 +374,8 @@ static void split(hctx* H, int* vs, int k, int lo, int depth) {
     /* the global adjacency is sorted and distinct, so local rows are too */
     int* cls = malloc(sizeof(int) * (size_t)k);
     int nls = hg_levelset(&g, cls);
+    const int nls_levelset = nls;
+    int ml_won = 0;
     int* side = malloc(sizeof(int) * (size_t)k);
     hg_bisect(&g, side);
     int bnd[2] = {0, 0};
@@ -388,6 +397,7 @@ static void split(hctx* H, int* vs, int k, int lo, int depth) {
     if (nml < nls && na_ml > 0 && nb_ml > 0) {
         for (int v = 0; v < k; v++) cls[v] = (isb[v] && side[v] == small) ? 2 : side[v];
         nls = nml;
+        ml_won = 1;
     }
     int* A = malloc(sizeof(int) * (size_t)k);
     int* B = malloc(sizeof(int) * (size_t)k);
@@ -405,6 +415,17 @@ static void split(hctx* H, int* vs, int k, int lo, int depth) {
     H->stats[1]++;
     H->stats[2] += ns;
     if (ns > H->stats[3]) H->stats[3] = ns;
+    if (H->trace && H->trace_n < H->trace_cap) {
+        int32_t* t = H->trace + kTraceFields * H->trace_n;
+        t[0] = lo;
+        t[1] = k;
+        t[2] = na;
+        t[3] = nb;
+        t[4] = ns;
+        t[5] = ml_won;
+        t[6] = nls_levelset;
+    }
+    if (H->trace) H->trace_n++;
     place(H, S, ns, lo + k - ns);
     if (na) solve(H, A, na, lo, depth + 1);
     if (nb) solve(H, B, nb, lo + na, depth + 1);
@@ -447,8 +468,9 @@ static void solve(hctx* H, int* vs, int k, int lo, int depth) {
     free(comp);
 }
 
-int or_order_hybrid(int32_t n, const int32_t* beg, const int32_t* end, const int32_t* col,
-                    int32_t leaf, int32_t* perm, int64_t* stats) {
+static int order_hybrid(int32_t n, const int32_t* beg, const int32_t* end, const int32_t* col,
+                        int32_t leaf, int32_t* perm, int64_t* stats, int32_t* trace,
+                        int64_t trace_cap, int64_t* trace_n) {
     if (n < 0 || leaf < 1 || (n > 0 && (!beg || !end || !perm))) return -1;
     if (stats) memset(stats, 0, 4 * sizeof(int64_t));
     if (n == 0) return 0;
@@ -488,15 +510,31 @@ int or_order_hybrid(int32_t n, const int32_t* beg, const int32_t* end, const int
     H.loc = malloc(sizeof(int) * (size_t)n);
     H.mark = calloc((size_t)n, sizeof(int));
     memset(H.stats, 0, sizeof(H.stats));
+    H.trace = trace;
+    H.trace_cap = trace_cap;
+    H.trace_n = 0;
     for (int32_t v = 0; v < n; v++) H.loc[v] = -1;
     int* all = malloc(sizeof(int) * (size_t)n);
     for (int32_t v = 0; v < n; v++) all[v] = v;
     solve(&H, all, n, 0, 0);
     if (stats) memcpy(stats, H.stats, sizeof(H.stats));
+    if (trace_n) *trace_n = H.trace_n;
     free(all);
     free(H.loc);
     free(H.mark);
     free(ptr);
     free(adj);
     return 0;
+}
+
+int or_order_hybrid(int32_t n, const int32_t* beg, const int32_t* end, const int32_t* col,
+                    int32_t leaf, int32_t* perm, int64_t* stats) {
+    return order_hybrid(n, beg, end, col, leaf, perm, stats, NULL, 0, NULL);
+}
+
+int or_order_hybrid_trace(int32_t n, const int32_t* beg, const int32_t* end, const int32_t* col,
+                          int32_t leaf, int32_t* perm, int64_t* stats, int32_t* trace,
+                          int64_t trace_cap, int64_t* trace_n) {
+    if (trace_cap < 0 || (trace_cap > 0 && !trace) || !trace_n) return -1;
+    return order_hybrid(n, beg, end, col, leaf, perm, stats, trace, trace_cap, trace_n);
 }

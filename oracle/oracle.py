@@ -42,6 +42,9 @@ def lib():
         L.or_free.argtypes = [vp]
         L.or_order_hybrid.restype = ctypes.c_int
         L.or_order_hybrid.argtypes = [ctypes.c_int32, vp, vp, vp, ctypes.c_int32, vp, vp]
+        L.or_order_hybrid_trace.restype = ctypes.c_int
+        L.or_order_hybrid_trace.argtypes = [ctypes.c_int32, vp, vp, vp, ctypes.c_int32, vp, vp,
+                                            vp, ctypes.c_int64, vp]
         L.or_order_nd.restype = ctypes.c_int
         L.or_order_nd.argtypes = [ctypes.c_int32, vp, vp, vp, ctypes.c_int32, ctypes.c_int32, vp,
                                   vp]
@@ -145,6 +148,27 @@ def order_hybrid(beg, end, col, leaf=32):
     if rc != 0:
         raise ValueError("oracle: bad ordering arguments")
     return perm[:n], tuple(int(x) for x in stats)
+
+
+def order_hybrid_trace(beg, end, col, leaf=32):
+    """order_hybrid, also returning every split: an int32 array of rows
+    (range start, component size, |A|, |B|, |S|, rule 0 level-set / 1
+    multilevel, the level-set separator's size).  The component's range holds
+    A, then B, then S."""
+    b = np.ascontiguousarray(beg, dtype=np.int32)
+    e = np.ascontiguousarray(end, dtype=np.int32)
+    c = np.ascontiguousarray(col, dtype=np.int32)
+    n = b.shape[0]
+    perm = np.zeros(max(n, 1), np.int32)
+    stats = np.zeros(4, np.int64)
+    cap = max(n, 1)
+    trace = np.zeros((cap, 7), np.int32)
+    cnt = np.zeros(1, np.int64)
+    rc = lib().or_order_hybrid_trace(n, _p(b), _p(e), _p(c), int(leaf), _p(perm), _p(stats),
+                                     _p(trace), cap, _p(cnt))
+    if rc != 0 or cnt[0] > cap:
+        raise ValueError("oracle: bad ordering arguments")
+    return perm[:n], tuple(int(x) for x in stats), trace[:int(cnt[0])]
 
 
 def read_dat(beg_file, end_file, csr_file):

@@ -40,6 +40,15 @@ def _sym_adj(beg, end, col):
     return adj
 
 
+def _sym_csr(beg, end, col):
+    """A + A^T as (row starts, neighbour ids): distinct, no loops."""
+    adj = _sym_adj(beg, end, col)
+    rp = np.zeros(len(adj) + 1, np.int64)
+    rp[1:] = np.cumsum([len(a) for a in adj])
+    flat = np.array([w for a in adj for w in sorted(a)], np.int64)
+    return rp, flat
+
+
 def nd_python(beg, end, col, leaf, max_rounds=512):
     """Level-set nested dissection, restated recursively from the rule:
     components in root order; a component above `leaf` is cut at the middle
@@ -313,22 +322,27 @@ def test_permute_then_factor(ctx):
 
 
 @pytest.mark.gpu
-def test_cli_order_mode(tmp_path):
-    """gsofa_cli --order: binary file -> device ordering -> P A P^T -> factor;
-    the fill equals the oracle's on the same permutation."""
+@pytest.mark.parametrize("mode", ["--order", "--order-hybrid"])
+def test_cli_order_mode(tmp_path, mode):
+    """gsofa_cli --order / --order-hybrid: binary file -> device ordering ->
+    P A P^T -> factor; the fill equals the oracle's on the same permutation."""
     import subprocess
     _cuda()
     from gsofatpds_b200 import _lib, write_binary
     b, e, c = _grid2d(50, 40, np.random.default_rng(9))
     path = str(tmp_path / "g.gsofacsr")
     write_binary(path, b, e, c)
-    out = subprocess.run([_lib.CLI_PATH, "--order", path, "128"], capture_output=True, text=True,
+    out = subprocess.run([_lib.CLI_PATH, mode, path, "128"], capture_output=True, text=True,
                          timeout=300)
     assert out.returncode == 0, out.stderr
-    perm, _ = O.order_nd(b, e, c, leaf=32)
+    if mode == "--order":
+        perm, _ = O.order_nd(b, e, c, leaf=32)
+    else:
+        perm, _ = O.order_hybrid(b, e, c, leaf=32)
     ref = _fill(*permuted(b, e, c, perm))
     assert "Final Number of fill-ins detected: %d" % ref in out.stdout, out.stdout
-    assert "Ordering (nested dissection on the device)" in out.stdout
+    rule = "level-set" if mode == "--order" else "hybrid"
+    assert "Ordering (%s nested dissection on the device)" % rule in out.stdout
 
 
 @pytest.mark.gpu
@@ -432,6 +446,60 @@ def test_hybrid_cuts_circuit_like_fill():
     f_l = _fill(*permuted(b, e, col, pl))
     f_h = _fill(*permuted(b, e, col, ph))
     assert f_h < f_l, (f_h, f_l)
+
+
+def _trace_graphs():
+    from gsofatpds_b200 import gen
+    from gsofatpds_b200.gen import csr_to_beg_end
+    rng = np.random.default_rng(41)
+    out = {}
+    n = 700
+    rows = [[int(j) for j in np.nonzero(rng.random(n) < 0.006)[0]] for _ in range(n)]
+    out["random"] = _csr(rows)
+    _, rp, col = gen_circuit(6000)
+    out["circuit"] = (*csr_to_beg_end(rp), col)
+    out["grid_scrambled"] = _grid2d(40, 30, rng)
+    return out
+
+
+@pytest.mark.parametrize("name", ["random", "circuit", "grid_scrambled"])
+def test_hybrid_oracle_splits_separate(name):
+    """Every split the hybrid oracle makes, checked on the permutation it
+    returns: the component's range holds A, B and S; no edge of A + A^T
+    joins A and B; a split with both sides non-empty has a separator; a
+    multilevel split is taken only when its separator is smaller than the
+    level-set one and leaves both sides non-empty, and each of its separator
+    vertices borders A or B; a level-set split keeps the level-set separator;
+    the statistics add up.  (The 40..60 % balance bounds each refinement move,
+    not the start that BFS growth gives on a weighted coarse graph, so the
+    final balance is not a property to assert.)"""
+    b, e, c = _trace_graphs()[name]
+    n = len(b)
+    perm, st, tr = O.order_hybrid_trace(b, e, c, leaf=8)
+    assert sorted(perm.tolist()) == list(range(n))
+    rp, adj = _sym_csr(b, e, c)
+    rule_seen = set()
+    for lo, k, na, nb, ns, rule, nls in tr.tolist():
+        assert na + nb + ns == k and ns >= 0
+        side = np.full(n, -1, np.int8)
+        side[perm[lo:lo + na]] = 0
+        side[perm[lo + na:lo + na + nb]] = 1
+        side[perm[lo + k - ns:lo + k]] = 2
+        for v in perm[lo:lo + na]:
+            assert not np.any(side[adj[rp[v]:rp[v + 1]]] == 1), (name, lo, v)
+        if na and nb:
+            assert ns > 0
+        if rule == 1:
+            assert ns < nls and na > 0 and nb > 0
+            for v in perm[lo + k - ns:lo + k]:
+                nb_sides = side[adj[rp[v]:rp[v + 1]]]
+                assert np.any((nb_sides == 0) | (nb_sides == 1)), (name, lo, v)
+        else:
+            assert ns == nls
+        rule_seen.add(rule)
+    assert st[1] == len(tr) and st[2] == int(tr[:, 4].sum()) and st[3] == int(tr[:, 4].max())
+    if name == "circuit":
+        assert 1 in rule_seen  # the multilevel rule wins somewhere on a small-world graph
 
 
 def gen_circuit(n):
