@@ -1111,6 +1111,26 @@ __global__ void __launch_bounds__(BLOCK, 1024 / BLOCK) traverse_kernel(TraverseL
                 if (dir == 0 && xl) {
                     if (xl == ~0u) {
                         c_e += (unsigned long long)ld_i32<CG>(M.wdeg + w);
+                    } else if (BLOCK >= 256 && lo_m == ~0u && __popc(xl) >= 28) {
+                        // a nearly full word (dense closures): its sum minus
+                        // the degrees of its at most four clear bits, every
+                        // load issued together, instead of three rounds of
+                        // bit-plane loads.  Not compiled into 128-thread CTAs
+                        // (small matrices, sparse closures), which measured
+                        // slower with it.
+                        uint32_t t = ~xl;
+                        int ra[4], rb[4];
+#pragma unroll
+                        for (int j = 0; j < 4; j++) {
+                            const int v = t ? (int)(base + __ffs(t) - 1) : -1;
+                            t &= t - 1;
+                            ra[j] = v >= 0 ? ld_i32<CG>(M.rowptr + v) : 0;
+                            rb[j] = v >= 0 ? ld_i32<CG>(M.rowptr + v + 1) : 0;
+                        }
+                        int d = ld_i32<CG>(M.wdeg + w);
+#pragma unroll
+                        for (int j = 0; j < 4; j++) d -= (rb[j] & ~3) - (ra[j] & ~3) - (rb[j] & 3);
+                        c_e += (unsigned long long)d;
                     } else if (__popc(xl) <= 2 || M.dplanes == nullptr) {
                         uint32_t t = xl;
                         while (t) {
