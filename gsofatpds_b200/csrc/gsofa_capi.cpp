@@ -335,8 +335,14 @@ int run_factor(gsofa_ctx* ctx, const gsofa_matrix* const* mats, int32_t count,
     LaunchCfg cfg;
     int rc = plan_launch(ctx, std::max(nmax, 1), o, &cfg);
     if (rc) return rc;
-    const long long chunk =
-        o->chunk_sources > 0 ? o->chunk_sources : default_chunk(total_sources, cfg.grid);
+    // So few sources that each can have a CTA of its own: chunks of one source
+    // run them all at once (a 115-row matrix: 0.06 instead of 0.23 ms); with
+    // more, chunks share closures between consecutive sources.
+    long long one_each = 0;
+    for (int32_t i = 0; i < count; i++) one_each += 2ll * mats[i]->n;
+    const long long chunk = o->chunk_sources > 0 ? o->chunk_sources
+                            : one_each <= cfg.grid ? 1
+                                                   : default_chunk(total_sources, cfg.grid);
     for (int32_t i = 0; i < count; i++) items += 2ll * ((mats[i]->n + chunk - 1) / chunk);
     rc = ensure(ctx, &ctx->queue, &ctx->queue_bytes, (size_t)cfg.grid * (size_t)std::max(nmax, 1) * 4);
     if (rc) return rc;
