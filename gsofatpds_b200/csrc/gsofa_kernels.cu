@@ -207,70 +207,122 @@ __device__ __forceinline__ uint32_t hset_insert(int w) {
     return 0u;
 }
 
-// Top-down visit of edge v -> w.  Returns true when w is a new vertex < src
-// to queue.  w == src (also the sentinel of idle lanes and the padding of the
-// source's row) is a no-op.  raw / orig count the source row's entries > src
-// (with multiplicity / distinct) for the reference's nz_row_U counter.
-__device__ __forceinline__ bool td_edge(const Src& S, int v, int w, uint32_t& raw, uint32_t& orig,
-                                        int& wl, int& wh) {
-    if (w == S.src) return false;
-    const uint32_t bit = 1u << (w & 31);
-    uint32_t* word = S.bm + (w >> 5);
-    bool fresh = false;
-    if (!(ld_vol(word) & bit)) fresh = !(atomicOr(word, bit) & bit);
-    if (fresh) {  // the set bits' word range (census and ring copy)
-        wl = min(wl, w >> 5);
-        wh = max(wh, w >> 5);
-    }
-    if (w > S.src) {
-        if (v == S.src) {
-            raw++;
-            if (S.chained) orig += hset_insert(w);
-            else if (fresh) orig++;
-        }
-        return false;
-    }
-    if (fresh && w >= S.cache_lo && !((S.merged_mask >> (w & (S.ring - 1))) & 1u)) {
-        atomicOr(S.reached, 1ull << (w & (S.ring - 1)));
-        *(volatile int*)S.abort_flag = 1;
-    }
-    return fresh;
-}
-
 // Warp-aggregated append of up to 4 vertices per lane to the queue.
+// BALLOT: one ballot per entry position gives each lane its offsets, and the
+// queue takes position 0 of all lanes, then position 1, and so on; otherwise
+// an inclusive shuffle scan of the per-lane counts keeps each lane's entries
+// together.  The queue's order does not change what a search reaches; the
+// ballot form measured faster with 512 threads per source and more (the
+// circuit-like n=659,033 matrix: 403 -> 366 ms), the scan with 128 and 256
+// (the 512-matrix grid/banded mix, 129 against 156 ms; the 64^3 grid, 5.2
+// against 5.4 ms).
+template <bool BALLOT>
 __device__ __forceinline__ void push4(int32_t* q, long long qcap, long long le, int* cnt,
                                       int32_t* status, int lane, const int4& e, unsigned f) {
-    const int mine = __popc(f);
-    if (!__any_sync(FULL_MASK, mine)) return;
-    int incl = mine;
+    if constexpr (BALLOT) {
+        if (!__any_sync(FULL_MASK, f)) return;
+        const unsigned b0 = __ballot_sync(FULL_MASK, f & 1u), b1 = __ballot_sync(FULL_MASK, f & 2u);
+        const unsigned b2 = __ballot_sync(FULL_MASK, f & 4u), b3 = __ballot_sync(FULL_MASK, f & 8u);
+        const int n0 = __popc(b0), n1 = __popc(b1), n2 = __popc(b2), n3 = __popc(b3);
+        const int total = n0 + n1 + n2 + n3;
+        int base = 0;
+        if (lane == 0) base = atomicAdd(cnt, total);
+        base = __shfl_sync(FULL_MASK, base, 0);
+        const unsigned lt = (1u << lane) - 1u;
+        const long long at0 = le + base;
+        const int ws[4] = {e.x, e.y, e.z, e.w};
+        const unsigned bs[4] = {b0, b1, b2, b3};
+        const int off[4] = {0, n0, n0 + n1, n0 + n1 + n2};
 #pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-        const int t = __shfl_up_sync(FULL_MASK, incl, o);
-        if (lane >= o) incl += t;
-    }
-    const int total = __shfl_sync(FULL_MASK, incl, 31);
-    int base = 0;
-    if (lane == 31) base = atomicAdd(cnt, total);
-    base = __shfl_sync(FULL_MASK, base, 31);
-    long long at = le + base + (incl - mine);
-    const int ws[4] = {e.x, e.y, e.z, e.w};
+        for (int c = 0; c < 4; c++) {
+            if (f & (1u << c)) {
+                const long long at = at0 + off[c] + __popc(bs[c] & lt);
+                if (at < qcap) q[at] = ws[c];
+                else atomicOr(status, DEV_ERR_QUEUE);
+            }
+        }
+    } else {
+        const int mine = __popc(f);
+        if (!__any_sync(FULL_MASK, mine)) return;
+        int incl = mine;
 #pragma unroll
-    for (int c = 0; c < 4; c++) {
-        if (f & (1u << c)) {
-            if (at < qcap) q[at] = ws[c];
-            else atomicOr(status, DEV_ERR_QUEUE);
-            at++;
+        for (int o = 1; o < 32; o <<= 1) {
+            const int t = __shfl_up_sync(FULL_MASK, incl, o);
+            if (lane >= o) incl += t;
+        }
+        const int total = __shfl_sync(FULL_MASK, incl, 31);
+        int base = 0;
+        if (lane == 31) base = atomicAdd(cnt, total);
+        base = __shfl_sync(FULL_MASK, base, 31);
+        long long at = le + base + (incl - mine);
+        const int ws[4] = {e.x, e.y, e.z, e.w};
+#pragma unroll
+        for (int c = 0; c < 4; c++) {
+            if (f & (1u << c)) {
+                if (at < qcap) q[at] = ws[c];
+                else atomicOr(status, DEV_ERR_QUEUE);
+                at++;
+            }
         }
     }
 }
 
+// Top-down visit of edges v -> e.x, e.y, e.z, e.w.  Bit c of the result is
+// set when entry c is a new vertex < src to queue.  An entry equal to src
+// (also the sentinel of idle lanes and the padding of the source's row) is a
+// no-op.  raw / orig count the source row's entries > src (with multiplicity
+// / distinct) for the reference's nz_row_U counter.
+template <bool PAIRED>
 __device__ __forceinline__ unsigned td_edge4(const Src& S, int v, const int4& e, uint32_t& raw,
                                              uint32_t& orig, int& wl, int& wh) {
+    // PAIRED: the bitmap accesses are issued four at a time: the four words
+    // are read together, then the unset bits are claimed together, so a lane
+    // waits for one read and one atomic rather than for four of each in turn.
+    // Two entries with the same bit stay correct: a thread's atomics on one
+    // word are ordered, and the second sees the first's bit.  Otherwise each
+    // entry's read and claim finish before the next entry's start.
+    const int ws[4] = {e.x, e.y, e.z, e.w};
+    uint32_t cur[4], old[4];
+    if constexpr (PAIRED) {
+#pragma unroll
+        for (int c = 0; c < 4; c++) cur[c] = ws[c] != S.src ? ld_vol(S.bm + (ws[c] >> 5)) : ~0u;
+#pragma unroll
+        for (int c = 0; c < 4; c++) {
+            const uint32_t bit = 1u << (ws[c] & 31);
+            old[c] = !(cur[c] & bit) ? atomicOr(S.bm + (ws[c] >> 5), bit) : bit;
+        }
+    } else {
+#pragma unroll
+        for (int c = 0; c < 4; c++) {
+            const uint32_t bit = 1u << (ws[c] & 31);
+            cur[c] = ws[c] != S.src ? ld_vol(S.bm + (ws[c] >> 5)) : ~0u;
+            old[c] = !(cur[c] & bit) ? atomicOr(S.bm + (ws[c] >> 5), bit) : bit;
+        }
+    }
     unsigned f = 0;
-    if (td_edge(S, v, e.x, raw, orig, wl, wh)) f |= 1u;
-    if (td_edge(S, v, e.y, raw, orig, wl, wh)) f |= 2u;
-    if (td_edge(S, v, e.z, raw, orig, wl, wh)) f |= 4u;
-    if (td_edge(S, v, e.w, raw, orig, wl, wh)) f |= 8u;
+#pragma unroll
+    for (int c = 0; c < 4; c++) {
+        const int w = ws[c];
+        if (w == S.src) continue;
+        const bool fresh = !(old[c] & (1u << (w & 31)));
+        if (fresh) {
+            wl = min(wl, w >> 5);
+            wh = max(wh, w >> 5);
+        }
+        if (w > S.src) {
+            if (v == S.src) {
+                raw++;
+                if (S.chained) orig += hset_insert(w);
+                else if (fresh) orig++;
+            }
+            continue;
+        }
+        if (fresh && w >= S.cache_lo && !((S.merged_mask >> (w & (S.ring - 1))) & 1u)) {
+            atomicOr(S.reached, 1ull << (w & (S.ring - 1)));
+            *(volatile int*)S.abort_flag = 1;
+        }
+        if (fresh) f |= 1u << c;
+    }
     return f;
 }
 
@@ -341,8 +393,8 @@ __device__ __forceinline__ void td_level(const Src& S, int32_t* q, long long qca
             for (int k0 = 0; k0 < hl; k0 += 128) {
                 const int kn = k0 + 128 + 4 * lane;
                 const int4 hn = kn < hl ? ld_row4<CG>(S.cl + hb + kn) : idle;
-                const unsigned f = td_edge4(S, hv, he, raw, orig, wl, wh);
-                push4(q, qcap, le, cnt, status, lane, he, f);
+                const unsigned f = td_edge4<(BLOCK >= 512)>(S, hv, he, raw, orig, wl, wh);
+                push4<(BLOCK >= 512)>(q, qcap, le, cnt, status, lane, he, f);
                 he = hn;
             }
         }
@@ -355,8 +407,8 @@ __device__ __forceinline__ void td_level(const Src& S, int32_t* q, long long qca
         int4 e = 0 < its ? ld_row4<CG>(S.cl + s0) : idle;
         for (int it = 0; it < maxit; it++) {
             const int4 nx = it + 1 < its ? ld_row4<CG>(S.cl + s0 + 4 * (it + 1)) : idle;
-            const unsigned f = td_edge4(S, v, e, raw, orig, wl, wh);
-            push4(q, qcap, le, cnt, status, lane, e, f);
+            const unsigned f = td_edge4<(BLOCK >= 512)>(S, v, e, raw, orig, wl, wh);
+            push4<(BLOCK >= 512)>(q, qcap, le, cnt, status, lane, e, f);
             e = nx;
         }
     }
