@@ -505,3 +505,56 @@ def test_hybrid_oracle_splits_separate(name):
 def gen_circuit(n):
     from gsofatpds_b200 import gen
     return gen.circuit_like(n=n, target_nnz=int(5830000 * n / 659033), seed=2)
+
+
+@pytest.mark.parametrize("nx,ny", [(3, 3), (4, 4), (5, 3)])
+def test_hybrid_grid_known_answer(nx, ny):
+    """Hand-worked: on an nx x ny 5-point grid (vertex i*ny + j) the search
+    for a pseudo-peripheral start ends at a corner, the level sets from a
+    corner are the anti-diagonals i + j = d, and the middle one,
+    d = (nx + ny - 2) // 2, is the top separator: no multilevel separator of
+    a grid this small is smaller, so the hybrid keeps it.  It is ordered
+    last; the two triangles it cuts off come first."""
+    b, e, c = _grid2d(nx, ny)
+    n = nx * ny
+    perm, _, tr = O.order_hybrid_trace(b, e, c, leaf=1)
+    d = (nx + ny - 2) // 2
+    diag = {i * ny + j for i in range(nx) for j in range(ny) if i + j == d}
+    near = {i * ny + j for i in range(nx) for j in range(ny) if i + j < d}
+    far = {i * ny + j for i in range(nx) for j in range(ny) if i + j > d}
+    k = len(diag)
+    assert set(perm[n - k:].tolist()) == diag
+    assert len(near) == len(far)  # the middle level of these shapes halves the rest
+    halves = {frozenset(perm[:len(near)].tolist()), frozenset(perm[len(near):n - k].tolist())}
+    assert halves == {frozenset(near), frozenset(far)}
+    lo, kk, na, nb, ns, rule, nls = tr[0].tolist()
+    assert (lo, kk, ns, rule, nls) == (0, n, k, 0, k)
+    pl, _ = O.order_nd(b, e, c, leaf=1)
+    assert np.array_equal(perm, pl)
+
+
+def test_hybrid_barbell_known_answer():
+    """Hand-worked: two 5-cliques joined through one bridge vertex.  The bridge
+    is the only one-vertex separator, so it is ordered last, with each clique
+    whole on one side before it.  A clique cannot be split, so inside each
+    the splits peel one vertex off as the separator."""
+    m = 5
+    rows = [[] for _ in range(2 * m + 1)]
+    for a in range(m):
+        for c in range(m):
+            if a != c:
+                rows[a].append(c)
+                rows[m + 1 + a].append(m + 1 + c)
+    rows[m - 1].append(m)
+    rows[m] += [m - 1, m + 1]
+    rows[m + 1].append(m)
+    b, e, c = _csr([sorted(r) for r in rows])
+    perm, _, tr = O.order_hybrid_trace(b, e, c, leaf=1)
+    assert perm[-1] == m
+    first, second = set(perm[:m].tolist()), set(perm[m:2 * m].tolist())
+    cliques = {frozenset(range(m)), frozenset(range(m + 1, 2 * m + 1))}
+    assert {frozenset(first), frozenset(second)} == cliques
+    assert tr[0].tolist()[:5] == [0, 2 * m + 1, m, m, 1]
+    for lo, k, na, nb, ns, rule, nls in tr[1:].tolist():
+        if k > 1:
+            assert ns >= 1 and min(na, nb) == 0, (lo, k, na, nb, ns)
