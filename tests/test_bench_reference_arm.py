@@ -51,3 +51,29 @@ def test_roofline_entry():
     assert abs(r["inspected_edges_per_s"] - 63747717944 / 0.87176) < 1.0
     r0 = bench.roofline_entry(10, 1, 4, 5, 1.0, 100.0, "fallback", None)
     assert r0["traffic"] is None and r0["achieved"] is None and r0["frac"] is None
+
+
+def test_roofline_traffic_matches_its_profile():
+    """The traffic the bench line reports is the committed ncu summary's
+    read + write bytes of one full-size traversal launch."""
+    import glob
+    import importlib.util
+    import re
+    spec = importlib.util.spec_from_file_location("bench_mod", os.path.join(ROOT, "bench.py"))
+    bench = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(bench)
+    seen = 0
+    for path in glob.glob(os.path.join(ROOT, "profiles", "traverse_*.md")):
+        text = open(path).read()
+        if "dram_bytes_per_launch:" not in text:
+            continue
+        workload = os.path.basename(path)[len("traverse_"):-len(".md")]
+        rd = re.search(r"\| dram__bytes_read\.sum \| ([0-9,]+) B \|", text)
+        wr = re.search(r"\| dram__bytes_write\.sum \| ([0-9,]+) B \|", text)
+        assert rd and wr, path
+        total = int(rd.group(1).replace(",", "")) + int(wr.group(1).replace(",", ""))
+        assert bench.read_traffic(workload) == total, (path, total)
+        seen += 1
+    assert seen >= 1
+    roof = bench.roofline_entry(1e12, 1e9, 1e10, 1000, 500.0, 6450.9, "measured", 3.2e11)
+    assert abs(roof["achieved"] - 640.0) < 1e-6 and abs(roof["frac"] - 640.0 / 6450.9) < 1e-12
